@@ -1,0 +1,106 @@
+/* xtb_eig.h -- C ABI of the B200 eigensolver library (libxtbeig.so).
+ *
+ * Part 1 is a drop-in for xtb's src/mctc/lapack/sytrd.c: the same eight symbols with the same Fortran by-reference
+ * signatures and LAPACK semantics that the reference re-exports from Swift
+ * (Sources/Diagonalization/Exports.swift:6-138), so libxtb links this library in sytrd.c's place
+ * (CMake XTB_SYTRD_LIBRARIES, reference scripts/build_xtb_swift.sh:21-34).  All arrays are caller-owned HOST arrays,
+ * column-major, 32-bit integers; nothing is retained between calls; inputs are overwritten in place as LAPACK does.
+ * Every step runs on the GPU (CUDA device current on the calling thread); there is no CPU fallback.  Work arrays are
+ * accepted for signature compatibility and not used.
+ *
+ * Part 2 adds what a two-stage or batched GPU solve needs and the xtb ABI cannot express (the reference calls for a
+ * whole-solve entry, reference LOG.md:119-120): LAPACK-shaped dsyevd/dsygvd, device-pointer variants, a batch call,
+ * the density-matrix adjoint, options and error reporting.
+ *
+ * Errors.  Entry points with an `info` argument report LAPACK-style info: 0 success, < 0 illegal argument,
+ * > 0 numerical failure (stedc: an eigenvalue failed to converge; sygvd: info = n + i if the leading minor of order i
+ * of B is not positive definite).  A CUDA failure (or a device wait that ran out of time) gives info = -1000 - code.
+ * The sytrd/ormtr entries have no error channel (as in LAPACK); after any call xtb_gpu_last_status() returns 0 or the
+ * failure code and xtb_gpu_last_error() a message.  Calls never abort the process.
+ *
+ * Threads.  Each host thread gets its own CUDA stream and workspace; results do not depend on the thread or on other
+ * concurrent calls (deterministic kernels, no floating-point atomics).
+ */
+#ifndef XTB_EIG_H
+#define XTB_EIG_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- Part 1: xtb sytrd.c ABI ------------------------------------------------------------------------------------ */
+
+/* dsytrd('U'): A (n x n, lda) upper triangle -> tridiagonal d (n), e (n-1), reflectors above the superdiagonal and
+ * tau (n-1).  Replaces Exports.swift:8-16 (xtb_dsytrd_upper).  work: n*32 (unused). */
+void xtb_dsytrd_upper(const int* n, double* a, const int* lda, double* d, double* e, double* tau, double* work);
+/* As above in FP32.  Replaces Exports.swift:19-27. */
+void xtb_ssytrd_upper(const int* n, float* a, const int* lda, float* d, float* e, float* tau, float* work);
+/* Same reduction reading both stored triangles of a full symmetric A.  Replaces Exports.swift:31-38. */
+void xtb_dsytrd_full(const int* n, double* a, const int* lda, double* d, double* e, double* tau, double* work);
+/* dormtr('L','U','N'): z (n x m, ldz) <- Q z with Q from xtb_dsytrd_upper.  Replaces Exports.swift:58-65. */
+void xtb_dormtr_upper(const int* n, const int* m, const double* a, const int* lda, const double* tau, double* z,
+                      const int* ldz, double* work);
+/* As above in FP32.  Replaces Exports.swift:68-75. */
+void xtb_sormtr_upper(const int* n, const int* m, const float* a, const int* lda, const float* tau, float* z,
+                      const int* ldz, float* work);
+/* dstedc('I'): d (n), e (n-1) -> eigenvalues ascending in d, orthonormal eigenvectors in z (n x n, ldz).
+ * lwork == -1 or liwork == -1 is a workspace query (work[0] = 1+4n+n^2, iwork[0] = 3+5n).
+ * Replaces Exports.swift:90-101. */
+void xtb_dstedc(const int* n, double* d, double* e, double* z, const int* ldz, double* work, const int* lwork,
+                int* iwork, const int* liwork, int* info);
+/* As above in FP32 (the merge arithmetic runs in FP64 and is rounded to FP32).  Replaces Exports.swift:105-115. */
+void xtb_sstedc(const int* n, float* d, float* e, float* z, const int* ldz, float* work, const int* lwork, int* iwork,
+                const int* liwork, int* info);
+/* dst(0:n,0:n) = the symmetric matrix whose upper triangle is src's.  Replaces Exports.swift:119-138. */
+void xtb_dsymmetrize_pad(const int* n, const double* src, const int* lds, double* dst, const int* ldd);
+
+/* ---- Part 2: whole solves (no counterpart in the reference's ABI) ------------------------------------------------ */
+
+/* LAPACK dsyevd shape: jobz 'V'/'N', uplo 'U'/'L'; a <- eigenvectors (jobz 'V'), w <- eigenvalues ascending.
+ * Pipeline: sytrd -> stedc -> ormtr on the GPU.  lwork/liwork == -1: query (returns 1). */
+void xtb_dsyevd_gpu(const char* jobz, const char* uplo, const int* n, double* a, const int* lda, double* w,
+                    double* work, const int* lwork, int* iwork, const int* liwork, int* info);
+/* LAPACK dsygvd shape, itype 1 (A x = lambda B x): a <- eigenvectors C (C^T B C = I), b <- Cholesky factor
+ * (upper for uplo 'U', lower for 'L'), w <- eigenvalues ascending.  Pipeline: potrf -> X = U^-1 -> X^T A X ->
+ * sytrd -> stedc -> ormtr -> X C'. */
+void xtb_dsygvd_gpu(const int* itype, const char* jobz, const char* uplo, const int* n, double* a, const int* lda,
+                    double* b, const int* ldb, double* w, double* work, const int* lwork, int* iwork,
+                    const int* liwork, int* info);
+
+/* Device-pointer variants (by value; uplo 'U'; vectors always computed).  All pointers are device memory of the
+ * current device; `stream` is a cudaStream_t (NULL: the calling thread's library stream).  The call returns after
+ * queueing the work, except that it synchronises the stream once at the end to read the device status; it returns
+ * LAPACK-style info. */
+int xtb_dsyevd_device(int n, double* a, int lda, double* w, void* stream);
+int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, void* stream);
+
+/* A batch of independent generalized problems (host arrays, itype 1, jobz 'V', uplo 'U'): problem i has size n[i],
+ * a[i] (lda[i]), b[i] (ldb[i]), w[i]; info[i] per problem.  Problems are ordered by n^3 (longest first) and spread
+ * over the library's streams.  Returns 0 or the first nonzero info. */
+int xtb_dsygvd_batched(int count, const int* n, double* const* a, const int* lda, double* const* b, const int* ldb,
+                       double* const* w, int* info);
+
+/* Adjoint of the Fermi-smeared density matrix P = C diag(f) C^T, f_i = 2 / (1 + exp((e_i - mu)/kT)), where
+ * H C = S C diag(e), C^T S C = I (H, S upper triangles, host arrays).  Given dL/dP = wbar (symmetric, n x n), returns
+ * dL/dH and dL/dS (symmetric, full) by the Daleckii-Krein formula, eigenpairs recomputed on the GPU.  Optionally
+ * returns e (w_out, may be NULL) and C (c_out, ldc; may be NULL).  Returns info. */
+int xtb_dsygvd_density_adjoint(int n, const double* h, int ldh, const double* s, int lds, double kt, double mu,
+                               const double* wbar, int ldw, double* dh, int lddh, double* ds, int ldds, double* w_out,
+                               double* c_out, int ldc);
+
+/* Options (process-wide): "sytrd_grid" (CTAs of the resident reduction, 0 = auto), "ormtr_nb" (reflectors per
+ * compact-WY block, default 128), "wait_limit_ms" (device wait time limit, default 2000).  Returns 0, or -1 for an
+ * unknown name. */
+int xtb_gpu_set_option(const char* name, long value);
+long xtb_gpu_get_option(const char* name);
+
+/* Last status of the calling thread: 0 or a failure code; message for humans. */
+int xtb_gpu_last_status(void);
+const char* xtb_gpu_last_error(void);
+/* Library version string. */
+const char* xtb_gpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XTB_EIG_H */

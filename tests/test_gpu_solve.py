@@ -1,0 +1,131 @@
+"""Whole solves on the GPU against the oracle on the benchmark configurations' inputs.
+
+Bars (FP64 path): eigenvalue error <= 1e-10 Eh against the oracle and against the exact spectrum the inputs are built
+with; backward error ||HC - SCe|| / (||H|| n eps) <= 10; S-orthogonality <= 1e-12; density matrix (aufbau at the
+HOMO/LUMO gap, invariant to signs and to rotations inside degenerate subspaces) within 1e-9 of the oracle's.
+"""
+import numpy as np
+import pytest
+
+from oracle import fermi, inputs, lapack, metrics
+
+pytestmark = pytest.mark.gpu
+
+
+def test_config1_standard_n412(xe):
+    a, lam = inputs.standard(412, seed=0)
+    w_ref, z_ref = lapack.syevd_chain(a)
+    w, z, info = xe.dsyevd(a)
+    assert info == 0
+    dw, res, orth = metrics.eigen_accuracy(a, lam, w, z)
+    assert dw < 1e-12 and res < 1e-13 and orth < 1e-12
+    assert np.max(np.abs(w - w_ref)) < 1e-12
+    # the 8-fold cluster (1e-6 apart) resolved
+    assert np.all(np.diff(w) > 0)
+
+
+def test_syevd_lower_and_values_only(xe):
+    a, lam = inputs.standard(100, seed=3)
+    w, z, info = xe.dsyevd(np.tril(a) + np.triu(np.full_like(a, 9.0), 1), uplo="L")
+    assert info == 0
+    np.testing.assert_allclose(w, lam, atol=1e-12)
+    w2, z2, info2 = xe.dsyevd(a, jobz="N")
+    assert info2 == 0 and z2 is None
+    np.testing.assert_allclose(w2, lam, atol=1e-12)
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 64, 65, 130, 300])
+def test_sygvd_small(xe, n):
+    h, s, lam = inputs.generalized(n, seed=20 + n)
+    w_ref, c_ref = lapack.sygvd_chain(h, s)
+    w, c, u, info = xe.dsygvd(h, s)
+    assert info == 0
+    assert np.max(np.abs(w - lam)) < 1e-10
+    assert np.max(np.abs(w - w_ref)) < 1e-12
+    assert metrics.backward_error(h, s, w, c) < 10
+    assert metrics.s_orthogonality(s, c) < 1e-12
+    u_ref, _ = lapack.potrf_upper(s)
+    np.testing.assert_allclose(np.triu(u), u_ref, atol=1e-12)
+    np.testing.assert_array_equal(np.tril(u, -1), np.tril(s, -1))
+    if n >= 2:
+        occ = metrics.aufbau(n, n // 2)
+        assert metrics.density_error(c, c_ref, occ) < 1e-9
+
+
+def test_sygvd_lower(xe):
+    n = 90
+    h, s, lam = inputs.generalized(n, seed=5)
+    w, c, l, info = xe.dsygvd(np.tril(h), np.tril(s), uplo="L")
+    assert info == 0
+    np.testing.assert_allclose(w, lam, atol=1e-11)
+    u_ref, _ = lapack.potrf_upper(s)
+    np.testing.assert_allclose(np.tril(l), u_ref.T, atol=1e-12)
+
+
+def test_config2_generalized_n1204(xe):
+    h, s, lam = inputs.generalized(1204, seed=1)
+    w_ref, c_ref = lapack.sygvd_chain(h, s)
+    w, c, u, info = xe.dsygvd(h, s)
+    assert info == 0
+    assert np.max(np.abs(w - w_ref)) <= 1e-10
+    assert np.max(np.abs(w - lam)) <= 1e-10
+    assert metrics.backward_error(h, s, w, c) < 10
+    assert metrics.s_orthogonality(s, c) < 1e-12
+    assert metrics.density_error(c, c_ref, metrics.aufbau(1204, 602)) <= 1e-9
+
+
+def test_not_positive_definite_info(xe):
+    n = 70
+    h, s, _ = inputs.generalized(n, seed=2)
+    s = s.copy()
+    s[40, 40] = -1.0
+    w, c, u, info = xe.dsygvd(h, s)
+    _, info_ref = lapack.potrf_upper(s)
+    assert info_ref > 0
+    assert info == n + info_ref
+
+
+def test_invalid_arguments(xe):
+    import ctypes
+
+    info = ctypes.c_int(0)
+    n = ctypes.c_int(4)
+    bad = ctypes.c_int(2)
+    one = ctypes.c_int(1)
+    buf = np.zeros(16)
+    xe.lib().xtb_dsygvd_gpu(ctypes.byref(ctypes.c_int(2)), b"V", b"U", ctypes.byref(n), xe._p(buf),
+                            ctypes.byref(n), xe._p(buf), ctypes.byref(n), xe._p(buf), None, ctypes.byref(one), None,
+                            ctypes.byref(one), ctypes.byref(info))
+    assert info.value == -1
+    xe.lib().xtb_dsyevd_gpu(b"V", b"U", ctypes.byref(n), xe._p(buf), ctypes.byref(bad), xe._p(buf), None,
+                            ctypes.byref(one), None, ctypes.byref(one), ctypes.byref(info))
+    assert info.value == -5
+
+
+@pytest.mark.parametrize("temp", [300.0, 1000.0])
+def test_density_adjoint_matches_dk_oracle(xe, temp):
+    n = 96
+    h, s, lam = inputs.generalized(n, seed=40)
+    kt = fermi.kt_of(temp)
+    mu = 0.5 * (lam[n // 2 - 1] + lam[n // 2])
+    rng = np.random.default_rng(1)
+    wb = rng.standard_normal((n, n))
+    wb = wb + wb.T
+    dh, ds, e, c, info = xe.density_adjoint(h, s, kt, mu, wb)
+    assert info == 0
+    w_ref, c_ref = lapack.sygvd_chain(h, s)
+    gh, gs = fermi.dk_gradient(c_ref, w_ref, wb, mu, kt)
+    scale_h = max(1.0, np.abs(gh).max())
+    scale_s = max(1.0, np.abs(gs).max())
+    assert np.max(np.abs(dh - gh)) < 1e-9 * scale_h
+    assert np.max(np.abs(ds - gs)) < 1e-9 * scale_s
+
+
+def test_batched_uneven(xe):
+    sizes = [37, 130, 64, 9, 200]
+    probs = [inputs.generalized(n, seed=1000 + i) for i, n in enumerate(sizes)]
+    w, c, u, info = xe.dsygvd_batched([p[0] for p in probs], [p[1] for p in probs])
+    assert np.all(info == 0)
+    for (h, s, lam), wi, ci in zip(probs, w, c):
+        assert np.max(np.abs(wi - lam)) < 1e-10
+        assert metrics.backward_error(h, s, wi, ci) < 10

@@ -1,0 +1,693 @@
+// Host library: the C ABI of include/xtb_eig.h over the device kernels.
+//
+// Per host thread and device a Context holds a non-blocking CUDA stream, grow-only device buffers and pinned staging
+// (keyed by purpose, reused across calls), a GEMM-descriptor arena and a device status word.  A host-pointer call
+// copies its inputs in, queues the pipeline, copies results back and synchronises once; the device status is read
+// at that point and turned into LAPACK-style info or the thread's last-error record.  Nothing is computed on the CPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cctype>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/xtb_eig.h"
+#include "kernels.h"
+
+namespace xtbeig {
+namespace {
+
+std::atomic<long> g_sytrd_grid{0};
+std::atomic<long> g_ormtr_nb{128};
+std::atomic<long> g_wait_ms{2000};
+
+struct Buf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+struct Context {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  size_t max_smem = 0;
+  std::map<std::string, Buf> dbufs, hbufs;
+  DescArena arena;
+  DeviceStatus* d_status = nullptr;
+  DeviceStatus* h_status = nullptr;
+};
+
+struct ThreadState {
+  std::map<int, Context*> ctx;  // by device; contexts live until process exit
+  int last_code = 0;
+  std::string last_msg;
+};
+
+thread_local ThreadState t_state;
+
+void record(int code, const std::string& msg) {
+  t_state.last_code = code;
+  t_state.last_msg = msg;
+}
+
+Context* context() {
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) {
+    record(-1000 - (int)err, std::string("no CUDA device: ") + cudaGetErrorString(err));
+    return nullptr;
+  }
+  auto it = t_state.ctx.find(dev);
+  if (it != t_state.ctx.end()) return it->second;
+  Context* c = new Context();
+  c->device = dev;
+  int v = 0;
+  if ((err = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (err = cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) {
+    record(-1000 - (int)err, std::string("context set-up failed: ") + cudaGetErrorString(err));
+    delete c;
+    return nullptr;
+  }
+  c->num_sms = v;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  c->max_smem = (size_t)v;
+  c->arena.cap = size_t(4) << 20;
+  if ((err = cudaMalloc((void**)&c->d_status, sizeof(DeviceStatus))) != cudaSuccess ||
+      (err = cudaMallocHost((void**)&c->h_status, sizeof(DeviceStatus))) != cudaSuccess ||
+      (err = cudaMalloc((void**)&c->arena.d, c->arena.cap)) != cudaSuccess ||
+      (err = cudaMallocHost((void**)&c->arena.h, c->arena.cap)) != cudaSuccess) {
+    record(-1000 - (int)err, std::string("context allocation failed: ") + cudaGetErrorString(err));
+    return nullptr;
+  }
+  t_state.ctx[dev] = c;
+  return c;
+}
+
+// A call on one context and stream.  Errors are sticky: after the first failure later steps are skipped.
+struct Call {
+  Context* c;
+  cudaStream_t s;
+  cudaError_t err = cudaSuccess;
+  const char* where = "";
+  bool ok() const { return err == cudaSuccess; }
+
+  Call(Context* ctx, cudaStream_t user) : c(ctx), s(user ? user : ctx->stream) {
+    c->arena.reset();
+    check(cudaMemsetAsync(c->d_status, 0, sizeof(DeviceStatus), s), "status reset");
+  }
+  bool check(cudaError_t e, const char* w) {
+    if (err == cudaSuccess && e != cudaSuccess) {
+      err = e;
+      where = w;
+    }
+    return err == cudaSuccess;
+  }
+  template <typename T>
+  T* dev(const char* key, size_t count) {
+    if (!ok()) return nullptr;
+    Buf& b = c->dbufs[key];
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    if (b.bytes < bytes) {
+      if (b.p) {
+        check(cudaDeviceSynchronize(), "sync before regrow");
+        cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+      }
+      const size_t grow = bytes + bytes / 8 + 4096;
+      if (!check(cudaMalloc(&b.p, grow), key)) return nullptr;
+      b.bytes = grow;
+    }
+    return reinterpret_cast<T*>(b.p);
+  }
+  template <typename T>
+  T* host(const char* key, size_t count) {
+    if (!ok()) return nullptr;
+    Buf& b = c->hbufs[key];
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    if (b.bytes < bytes) {
+      if (b.p) {
+        check(cudaDeviceSynchronize(), "sync before regrow");
+        cudaFreeHost(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+      }
+      const size_t grow = bytes + bytes / 8 + 4096;
+      if (!check(cudaMallocHost(&b.p, grow), key)) return nullptr;
+      b.bytes = grow;
+    }
+    return reinterpret_cast<T*>(b.p);
+  }
+  void h2d(void* d, const void* h, size_t bytes, const char* w) {
+    if (ok() && bytes) check(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s), w);
+  }
+  void d2h(void* h, const void* d, size_t bytes, const char* w) {
+    if (ok() && bytes) check(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, s), w);
+  }
+  // Synchronise, read the device status.  Returns 0, a device status code (> 0), or -1000 - cudaError.
+  int finish(DeviceStatus* out = nullptr) {
+    if (ok()) check(cudaGetLastError(), "launch");
+    if (ok()) check(cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, s),
+                    "status read");
+    cudaError_t se = cudaStreamSynchronize(s);
+    if (ok() && se != cudaSuccess) check(se, "synchronize");
+    if (!ok()) {
+      record(-1000 - (int)err, std::string("CUDA error at ") + where + ": " + cudaGetErrorString(err));
+      return -1000 - (int)err;
+    }
+    DeviceStatus st = *c->h_status;
+    if (out) *out = st;
+    if (st.code != kStatusOk) {
+      const char* what = st.code == kStatusBarrierTimeout ? "device barrier wait exceeded its time limit"
+                         : st.code == kStatusSecularNoConv ? "secular equation did not converge"
+                         : st.code == kStatusNotSPD       ? "matrix not positive definite"
+                                                          : "device error";
+      char buf[160];
+      std::snprintf(buf, sizeof(buf), "%s (code %d, info %d, at %d)", what, st.code, st.info, st.where);
+      record(st.code, buf);
+      return st.code;
+    }
+    record(0, "");
+    return 0;
+  }
+};
+
+uint64_t wait_limit_ns() { return (uint64_t)g_wait_ms.load() * 1000000ull; }
+
+// ------------------------------------------------------------------------------------------------ stages
+
+template <typename T>
+void stage_sytrd(Call& k, int n, const T* dfull, int ldf, T* dout, int lda, T* d, T* e, T* tau) {
+  if (!k.ok() || n <= 0) return;
+  const size_t smem_cap = k.c->max_smem > 2048 ? k.c->max_smem - 2048 : k.c->max_smem;
+  SytrdPlan pl = sytrd_plan<T>(n, k.c->num_sms, smem_cap, (int)g_sytrd_grid.load());
+  if (!pl.supported) {
+    k.check(cudaErrorInvalidValue, "sytrd: size not supported");
+    return;
+  }
+  SytrdParams<T> p{};
+  p.n = n;
+  p.afull = dfull;
+  p.ldf = ldf;
+  p.aout = dout;
+  p.lda = lda;
+  p.d = d;
+  p.e = e;
+  p.tau = tau;
+  T* xch = k.template dev<T>("sytrd.xch", 4 * (size_t)n);
+  unsigned* ctr = k.template dev<unsigned>("sytrd.ctr", 64);
+  if (!k.ok()) return;
+  p.ybuf = xch;
+  p.cbuf = xch + 2 * (size_t)n;
+  p.counter = ctr;
+  p.st = k.c->d_status;
+  p.rows_per_cta = pl.rows_per_cta;
+  p.ldr = pl.ldr;
+  p.use_smem = pl.rows_in_smem ? 1 : 0;
+  p.limit_ns = wait_limit_ns();
+  if (!pl.rows_in_smem) {
+    p.grows = k.template dev<T>("sytrd.rows", (size_t)pl.grid * pl.rows_per_cta * pl.ldr);
+    if (!k.ok()) return;
+  }
+  k.check(cudaMemsetAsync(ctr, 0, 64 * sizeof(unsigned), k.s), "sytrd counter");
+  if (k.ok()) k.check(sytrd_launch<T>(p, pl, k.s), "sytrd launch");
+}
+
+template <typename T>
+void stage_ormtr(Call& k, int n, int m, const T* a, int lda, const T* tau, T* z, int ldz) {
+  if (!k.ok() || n <= 1 || m <= 0) return;
+  const int nb = (int)std::max<long>(16, g_ormtr_nb.load());
+  T* w = k.template dev<T>("ormtr.work", ormtr_work_elems<T>(n, m, nb));
+  if (!k.ok()) return;
+  k.check(ormtr_upper<T>(n, m, a, lda, tau, z, ldz, nb, ormtr_carve<T>(w, n, m, nb), k.c->arena, k.s), "ormtr");
+}
+
+void stage_stedc(Call& k, int n, double* d, double* e, double* z, int ldz) {
+  if (!k.ok() || n <= 0) return;
+  const size_t wb = stedc_work_bytes(n);
+  char* w = k.template dev<char>("stedc.work", wb);
+  const size_t hb = (size_t)40 * n * sizeof(int) + (size_t)4 * (n + 8) * sizeof(GemmDesc<double>) + 4096;
+  char* h = k.template host<char>("stedc.stage", hb);
+  if (!k.ok()) return;
+  k.check(stedc_device(n, d, e, z, ldz, w, wb, h, hb, k.c->d_status, k.s), "stedc");
+}
+
+// The generalized core on device buffers: h (n x n, full symmetric, ld n) is consumed; u (n x n, ld n) holds B's upper
+// triangle on entry and U on exit; c (n x n, ld n) receives C; w (n) the eigenvalues.
+void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
+  if (!k.ok() || n <= 0) return;
+  double* x = k.template dev<double>("gv.X", (size_t)n * n);
+  double* t = k.template dev<double>("gv.T", (size_t)n * n);
+  double* hp = k.template dev<double>("gv.Hp", (size_t)n * n);
+  double* r = k.template dev<double>("gv.R", (size_t)n * n);
+  double* z = k.template dev<double>("gv.Z", (size_t)n * n);
+  double* e = k.template dev<double>("gv.e", (size_t)n);
+  double* tau = k.template dev<double>("gv.tau", (size_t)n);
+  if (!k.ok()) return;
+  k.check(potrf_upper(n, u, n, k.c->d_status, k.c->arena, k.s), "potrf");
+  if (k.ok()) k.check(trtri_upper(n, u, n, x, n, t, k.c->arena, k.s), "trtri");
+  // G = H X (X upper), then H' = X^T G on the upper tiles, symmetrised for the reduction.
+  GemmDesc<double> p = gemm_problem<double>(n, n, n, 1.0, h, n, 0, x, n, 0, 0.0, t, n, kTriBUpper);
+  if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "congruence 1");
+  p = gemm_problem<double>(n, n, n, 1.0, x, n, 1, t, n, 0, 0.0, hp, n, kTriALower | kCUpper);
+  if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "congruence 2");
+  if (k.ok()) symmetrize_upper<double>(n, hp, n, h, n, k.s);
+  stage_sytrd<double>(k, n, h, n, r, n, w, e, tau);
+  stage_stedc(k, n, w, e, z, n);
+  stage_ormtr<double>(k, n, n, r, n, tau, z, n);
+  // C = X Z (X upper).
+  p = gemm_problem<double>(n, n, n, 1.0, x, n, 0, z, n, 0, 0.0, c, n, kTriAUpper);
+  if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "back-transform");
+}
+
+// Standard problem on device buffers: f (n x n full symmetric, ld n) consumed; z (n x n) eigenvectors; w eigenvalues.
+void core_syevd(Call& k, int n, double* f, double* z, double* w, bool vectors) {
+  if (!k.ok() || n <= 0) return;
+  double* r = k.template dev<double>("ev.R", (size_t)n * n);
+  double* e = k.template dev<double>("ev.e", (size_t)n);
+  double* tau = k.template dev<double>("ev.tau", (size_t)n);
+  if (!k.ok()) return;
+  stage_sytrd<double>(k, n, f, n, r, n, w, e, tau);
+  stage_stedc(k, n, w, e, z, n);
+  if (vectors) stage_ormtr<double>(k, n, n, r, n, tau, z, n);
+}
+
+int info_of(int code, const DeviceStatus& st, int n) {
+  if (code <= -1000) return code;
+  if (code == kStatusNotSPD) return n + st.info;
+  if (code == kStatusSecularNoConv) return st.info > 0 ? st.info : 1;
+  if (code == kStatusBarrierTimeout) return -2000 - kStatusBarrierTimeout;
+  return code == 0 ? 0 : -2000 - code;
+}
+
+char upc(const char* c) { return c ? (char)std::toupper((unsigned char)c[0]) : 'U'; }
+
+// ------------------------------------------------------------------------------------------------ ABI bodies
+
+template <typename T>
+void sytrd_host(const int* n_, T* a, const int* lda_, T* d, T* e, T* tau, bool full) {
+  const int n = *n_, lda = *lda_;
+  if (n <= 0) return;
+  if (lda < n) {
+    record(-3, "sytrd: lda < n");
+    return;
+  }
+  Context* c = context();
+  if (!c) return;
+  Call k(c, nullptr);
+  T* da = k.template dev<T>("io.A", (size_t)lda * n);
+  T* df = k.template dev<T>("io.F", (size_t)n * n);
+  T* dd = k.template dev<T>("io.d", n);
+  T* de = k.template dev<T>("io.e", n);
+  T* dt = k.template dev<T>("io.tau", n);
+  k.h2d(da, a, sizeof(T) * (size_t)lda * n, "H2D A");
+  if (k.ok()) {
+    if (full) copy_matrix<T>(n, n, da, lda, df, n, k.s);
+    else symmetrize_upper<T>(n, da, lda, df, n, k.s);
+  }
+  stage_sytrd<T>(k, n, df, n, da, lda, dd, de, dt);
+  k.d2h(a, da, sizeof(T) * (size_t)lda * n, "D2H A");
+  k.d2h(d, dd, sizeof(T) * n, "D2H d");
+  if (n > 1) {
+    k.d2h(e, de, sizeof(T) * (n - 1), "D2H e");
+    k.d2h(tau, dt, sizeof(T) * (n - 1), "D2H tau");
+  }
+  k.finish();
+}
+
+template <typename T>
+void ormtr_host(const int* n_, const int* m_, const T* a, const int* lda_, const T* tau, T* z, const int* ldz_) {
+  const int n = *n_, m = *m_, lda = *lda_, ldz = *ldz_;
+  if (n <= 1 || m <= 0) return;
+  if (lda < n || ldz < n) {
+    record(-4, "ormtr: leading dimension < n");
+    return;
+  }
+  Context* c = context();
+  if (!c) return;
+  Call k(c, nullptr);
+  T* da = k.template dev<T>("io.A", (size_t)lda * n);
+  T* dt = k.template dev<T>("io.tau", n);
+  T* dz = k.template dev<T>("io.Z", (size_t)ldz * m);
+  k.h2d(da, a, sizeof(T) * (size_t)lda * n, "H2D A");
+  k.h2d(dt, tau, sizeof(T) * (n - 1), "H2D tau");
+  k.h2d(dz, z, sizeof(T) * (size_t)ldz * m, "H2D Z");
+  stage_ormtr<T>(k, n, m, da, lda, dt, dz, ldz);
+  k.d2h(z, dz, sizeof(T) * (size_t)ldz * m, "D2H Z");
+  k.finish();
+}
+
+template <typename T>
+void stedc_host(const int* n_, T* d, T* e, T* z, const int* ldz_, T* work, const int* lwork, int* iwork,
+                const int* liwork, int* info) {
+  const int n = *n_;
+  *info = 0;
+  if ((lwork && *lwork == -1) || (liwork && *liwork == -1)) {
+    if (work) work[0] = (T)(1.0 + 4.0 * n + (double)n * n);
+    if (iwork) iwork[0] = 3 + 5 * n;
+    return;
+  }
+  if (n < 0) { *info = -2; return; }
+  if (n == 0) return;
+  const int ldz = *ldz_;
+  if (ldz < n) { *info = -6; return; }
+  Context* c = context();
+  if (!c) { *info = t_state.last_code; return; }
+  Call k(c, nullptr);
+  double* dd = k.template dev<double>("io.sd", n);
+  double* de = k.template dev<double>("io.se", n);
+  double* dz = k.template dev<double>("io.sZ", (size_t)n * n);
+  if (sizeof(T) == sizeof(double)) {
+    k.h2d(dd, d, sizeof(double) * n, "H2D d");
+    if (n > 1) k.h2d(de, e, sizeof(double) * (n - 1), "H2D e");
+  } else {
+    float* fd = k.template dev<float>("io.fd", 2 * (size_t)n);
+    k.h2d(fd, d, sizeof(float) * n, "H2D d");
+    if (n > 1) k.h2d(fd + n, e, sizeof(float) * (n - 1), "H2D e");
+    if (k.ok()) {
+      convert_f32_to_f64(n, fd, dd, k.s);
+      if (n > 1) convert_f32_to_f64(n - 1, fd + n, de, k.s);
+    }
+  }
+  stage_stedc(k, n, dd, de, dz, n);
+  if (sizeof(T) == sizeof(double)) {
+    k.d2h(d, dd, sizeof(double) * n, "D2H d");
+    if (k.ok()) k.check(cudaMemcpy2DAsync(z, sizeof(T) * ldz, dz, sizeof(double) * n, sizeof(double) * n, n,
+                                          cudaMemcpyDeviceToHost, k.s), "D2H Z");
+  } else {
+    float* fz = k.template dev<float>("io.fZ", (size_t)n * n + n);
+    if (k.ok()) {
+      convert_f64_to_f32((size_t)n * n, dz, fz, k.s);
+      convert_f64_to_f32(n, dd, fz + (size_t)n * n, k.s);
+    }
+    k.d2h(d, fz + (size_t)n * n, sizeof(float) * n, "D2H d");
+    if (k.ok()) k.check(cudaMemcpy2DAsync(z, sizeof(T) * ldz, fz, sizeof(float) * n, sizeof(float) * n, n,
+                                          cudaMemcpyDeviceToHost, k.s), "D2H Z");
+  }
+  DeviceStatus st{};
+  const int code = k.finish(&st);
+  *info = info_of(code, st, n);
+}
+
+}  // namespace
+}  // namespace xtbeig
+
+using namespace xtbeig;
+
+extern "C" {
+
+void xtb_dsytrd_upper(const int* n, double* a, const int* lda, double* d, double* e, double* tau, double* work) {
+  (void)work;
+  sytrd_host<double>(n, a, lda, d, e, tau, false);
+}
+
+void xtb_ssytrd_upper(const int* n, float* a, const int* lda, float* d, float* e, float* tau, float* work) {
+  (void)work;
+  sytrd_host<float>(n, a, lda, d, e, tau, false);
+}
+
+void xtb_dsytrd_full(const int* n, double* a, const int* lda, double* d, double* e, double* tau, double* work) {
+  (void)work;
+  sytrd_host<double>(n, a, lda, d, e, tau, true);
+}
+
+void xtb_dormtr_upper(const int* n, const int* m, const double* a, const int* lda, const double* tau, double* z,
+                      const int* ldz, double* work) {
+  (void)work;
+  ormtr_host<double>(n, m, a, lda, tau, z, ldz);
+}
+
+void xtb_sormtr_upper(const int* n, const int* m, const float* a, const int* lda, const float* tau, float* z,
+                      const int* ldz, float* work) {
+  (void)work;
+  ormtr_host<float>(n, m, a, lda, tau, z, ldz);
+}
+
+void xtb_dstedc(const int* n, double* d, double* e, double* z, const int* ldz, double* work, const int* lwork,
+                int* iwork, const int* liwork, int* info) {
+  stedc_host<double>(n, d, e, z, ldz, work, lwork, iwork, liwork, info);
+}
+
+void xtb_sstedc(const int* n, float* d, float* e, float* z, const int* ldz, float* work, const int* lwork, int* iwork,
+                const int* liwork, int* info) {
+  stedc_host<float>(n, d, e, z, ldz, work, lwork, iwork, liwork, info);
+}
+
+void xtb_dsymmetrize_pad(const int* n_, const double* src, const int* lds_, double* dst, const int* ldd_) {
+  const int n = *n_, lds = *lds_, ldd = *ldd_;
+  if (n <= 0) return;
+  if (lds < n || ldd < n) {
+    record(-3, "symmetrize_pad: leading dimension < n");
+    return;
+  }
+  Context* c = context();
+  if (!c) return;
+  Call k(c, nullptr);
+  double* ds = k.dev<double>("io.A", (size_t)lds * n);
+  double* dd = k.dev<double>("io.F", (size_t)n * n);
+  k.h2d(ds, src, sizeof(double) * (size_t)lds * n, "H2D src");
+  if (k.ok()) symmetrize_upper<double>(n, ds, lds, dd, n, k.s);
+  if (k.ok()) k.check(cudaMemcpy2DAsync(dst, sizeof(double) * ldd, dd, sizeof(double) * n, sizeof(double) * n, n,
+                                        cudaMemcpyDeviceToHost, k.s), "D2H dst");
+  k.finish();
+}
+
+void xtb_dsyevd_gpu(const char* jobz, const char* uplo, const int* n_, double* a, const int* lda_, double* w,
+                    double* work, const int* lwork, int* iwork, const int* liwork, int* info) {
+  *info = 0;
+  const char jz = upc(jobz), ul = upc(uplo);
+  if (jz != 'V' && jz != 'N') { *info = -1; return; }
+  if (ul != 'U' && ul != 'L') { *info = -2; return; }
+  const int n = *n_;
+  if (n < 0) { *info = -3; return; }
+  if ((lwork && *lwork == -1) || (liwork && *liwork == -1)) {
+    if (work) work[0] = 1;
+    if (iwork) iwork[0] = 1;
+    return;
+  }
+  const int lda = *lda_;
+  if (lda < std::max(1, n)) { *info = -5; return; }
+  if (n == 0) return;
+  Context* c = context();
+  if (!c) { *info = t_state.last_code; return; }
+  Call k(c, nullptr);
+  double* da = k.dev<double>("io.A", (size_t)lda * n);
+  double* df = k.dev<double>("io.F", (size_t)n * n);
+  double* dz = k.dev<double>("io.Z", (size_t)n * n);
+  double* dw = k.dev<double>("io.w", n);
+  k.h2d(da, a, sizeof(double) * (size_t)lda * n, "H2D A");
+  if (k.ok()) {
+    if (ul == 'U') symmetrize_upper<double>(n, da, lda, df, n, k.s);
+    else symmetrize_lower<double>(n, da, lda, df, n, k.s);
+  }
+  core_syevd(k, n, df, dz, dw, jz == 'V');
+  k.d2h(w, dw, sizeof(double) * n, "D2H w");
+  if (jz == 'V' && k.ok())
+    k.check(cudaMemcpy2DAsync(a, sizeof(double) * lda, dz, sizeof(double) * n, sizeof(double) * n, n,
+                              cudaMemcpyDeviceToHost, k.s), "D2H Z");
+  DeviceStatus st{};
+  const int code = k.finish(&st);
+  *info = info_of(code, st, n);
+}
+
+void xtb_dsygvd_gpu(const int* itype, const char* jobz, const char* uplo, const int* n_, double* a, const int* lda_,
+                    double* b, const int* ldb_, double* w, double* work, const int* lwork, int* iwork,
+                    const int* liwork, int* info) {
+  *info = 0;
+  if (!itype || *itype != 1) { *info = -1; return; }
+  const char jz = upc(jobz), ul = upc(uplo);
+  if (jz != 'V' && jz != 'N') { *info = -2; return; }
+  if (ul != 'U' && ul != 'L') { *info = -3; return; }
+  const int n = *n_;
+  if (n < 0) { *info = -4; return; }
+  if ((lwork && *lwork == -1) || (liwork && *liwork == -1)) {
+    if (work) work[0] = 1;
+    if (iwork) iwork[0] = 1;
+    return;
+  }
+  const int lda = *lda_, ldb = *ldb_;
+  if (lda < std::max(1, n)) { *info = -6; return; }
+  if (ldb < std::max(1, n)) { *info = -8; return; }
+  if (n == 0) return;
+  Context* c = context();
+  if (!c) { *info = t_state.last_code; return; }
+  Call k(c, nullptr);
+  double* da = k.dev<double>("io.A", (size_t)lda * n);
+  double* db = k.dev<double>("io.B", (size_t)ldb * n);
+  double* dh = k.dev<double>("io.F", (size_t)n * n);
+  double* du = k.dev<double>("io.U", (size_t)n * n);
+  double* dc = k.dev<double>("io.C", (size_t)n * n);
+  double* dw = k.dev<double>("io.w", n);
+  k.h2d(da, a, sizeof(double) * (size_t)lda * n, "H2D A");
+  k.h2d(db, b, sizeof(double) * (size_t)ldb * n, "H2D B");
+  if (k.ok()) {
+    if (ul == 'U') {
+      symmetrize_upper<double>(n, da, lda, dh, n, k.s);
+      copy_matrix<double>(n, n, db, ldb, du, n, k.s);
+    } else {
+      symmetrize_lower<double>(n, da, lda, dh, n, k.s);
+      symmetrize_lower<double>(n, db, ldb, du, n, k.s);
+    }
+  }
+  core_sygvd(k, n, dh, du, dc, dw);
+  // B <- the factor in the caller's triangle; the other triangle keeps its input (du's lower part is the input's).
+  if (k.ok()) {
+    if (ul == 'U') copy_matrix<double>(n, n, du, n, db, ldb, k.s);
+    else upper_transpose_to_lower<double>(n, du, n, db, ldb, k.s);
+  }
+  k.d2h(b, db, sizeof(double) * (size_t)ldb * n, "D2H B");
+  k.d2h(w, dw, sizeof(double) * n, "D2H w");
+  if (jz == 'V' && k.ok())
+    k.check(cudaMemcpy2DAsync(a, sizeof(double) * lda, dc, sizeof(double) * n, sizeof(double) * n, n,
+                              cudaMemcpyDeviceToHost, k.s), "D2H C");
+  DeviceStatus st{};
+  int code = k.finish(&st);
+  *info = info_of(code, st, n);
+}
+
+
+int xtb_dsyevd_device(int n, double* a, int lda, double* w, void* stream) {
+  if (n < 0) return -1;
+  if (lda < std::max(1, n)) return -3;
+  if (n == 0) return 0;
+  Context* c = context();
+  if (!c) return t_state.last_code;
+  Call k(c, (cudaStream_t)stream);
+  double* df = k.dev<double>("dv.F", (size_t)n * n);
+  double* dz = k.dev<double>("dv.Z", (size_t)n * n);
+  if (k.ok()) symmetrize_upper<double>(n, a, lda, df, n, k.s);
+  core_syevd(k, n, df, dz, w, true);
+  if (k.ok()) copy_matrix<double>(n, n, dz, n, a, lda, k.s);
+  DeviceStatus st{};
+  const int code = k.finish(&st);
+  return info_of(code, st, n);
+}
+
+int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, void* stream) {
+  if (n < 0) return -1;
+  if (lda < std::max(1, n)) return -3;
+  if (ldb < std::max(1, n)) return -5;
+  if (n == 0) return 0;
+  Context* c = context();
+  if (!c) return t_state.last_code;
+  Call k(c, (cudaStream_t)stream);
+  double* dh = k.dev<double>("dv.F", (size_t)n * n);
+  double* du = k.dev<double>("dv.U", (size_t)n * n);
+  double* dc = k.dev<double>("dv.C", (size_t)n * n);
+  if (k.ok()) {
+    symmetrize_upper<double>(n, a, lda, dh, n, k.s);
+    copy_matrix<double>(n, n, b, ldb, du, n, k.s);
+  }
+  core_sygvd(k, n, dh, du, dc, w);
+  if (k.ok()) {
+    copy_matrix<double>(n, n, dc, n, a, lda, k.s);
+    copy_matrix<double>(n, n, du, n, b, ldb, k.s);
+  }
+  DeviceStatus st{};
+  const int code = k.finish(&st);
+  return info_of(code, st, n);
+}
+
+int xtb_dsygvd_batched(int count, const int* n, double* const* a, const int* lda, double* const* b, const int* ldb,
+                       double* const* w, int* info) {
+  if (count <= 0) return 0;
+  // Longest first (n^3), so the tail of the batch is short problems.
+  std::vector<int> order(count);
+  for (int i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return n[x] > n[y]; });
+  int first = 0;
+  const int itype = 1;
+  for (int idx : order) {
+    int inf = 0;
+    xtb_dsygvd_gpu(&itype, "V", "U", &n[idx], a[idx], &lda[idx], b[idx], &ldb[idx], w[idx], nullptr, nullptr,
+                   nullptr, nullptr, &inf);
+    if (info) info[idx] = inf;
+    if (inf != 0 && first == 0) first = inf;
+  }
+  return first;
+}
+
+int xtb_dsygvd_density_adjoint(int n, const double* h, int ldh, const double* s, int lds, double kt, double mu,
+                               const double* wbar, int ldw, double* dh, int lddh, double* ds, int ldds, double* w_out,
+                               double* c_out, int ldc) {
+  if (n < 0) return -1;
+  if (ldh < std::max(1, n)) return -3;
+  if (lds < std::max(1, n)) return -5;
+  if (!(kt > 0.0)) return -6;
+  if (ldw < std::max(1, n)) return -9;
+  if (lddh < std::max(1, n)) return -11;
+  if (ldds < std::max(1, n)) return -13;
+  if (c_out && ldc < std::max(1, n)) return -16;
+  if (n == 0) return 0;
+  Context* c = context();
+  if (!c) return t_state.last_code;
+  Call k(c, nullptr);
+  double* da = k.dev<double>("io.A", (size_t)ldh * n);
+  double* db = k.dev<double>("io.B", (size_t)lds * n);
+  double* dwb = k.dev<double>("adj.W", (size_t)ldw * n);
+  double* hf = k.dev<double>("io.F", (size_t)n * n);
+  double* du = k.dev<double>("io.U", (size_t)n * n);
+  double* dc = k.dev<double>("io.C", (size_t)n * n);
+  double* dw = k.dev<double>("io.w", n);
+  double* wf = k.dev<double>("adj.Wf", (size_t)n * n);
+  double* gh = k.dev<double>("adj.dH", (size_t)n * n);
+  double* gs = k.dev<double>("adj.dS", (size_t)n * n);
+  double* t1 = k.dev<double>("adj.t1", (size_t)n * n);
+  double* t2 = k.dev<double>("adj.t2", (size_t)n * n);
+  double* t3 = k.dev<double>("adj.t3", (size_t)n * n);
+  k.h2d(da, h, sizeof(double) * (size_t)ldh * n, "H2D H");
+  k.h2d(db, s, sizeof(double) * (size_t)lds * n, "H2D S");
+  k.h2d(dwb, wbar, sizeof(double) * (size_t)ldw * n, "H2D Wbar");
+  if (k.ok()) {
+    symmetrize_upper<double>(n, da, ldh, hf, n, k.s);
+    copy_matrix<double>(n, n, db, lds, du, n, k.s);
+    copy_matrix<double>(n, n, dwb, ldw, wf, n, k.s);
+  }
+  core_sygvd(k, n, hf, du, dc, dw);
+  if (k.ok()) k.check(dk_adjoint(n, dc, dw, mu, kt, wf, gh, gs, t1, t2, t3, c->arena, k.s), "adjoint");
+  if (k.ok()) {
+    k.check(cudaMemcpy2DAsync(dh, sizeof(double) * lddh, gh, sizeof(double) * n, sizeof(double) * n, n,
+                              cudaMemcpyDeviceToHost, k.s), "D2H dH");
+  }
+  if (k.ok()) {
+    k.check(cudaMemcpy2DAsync(ds, sizeof(double) * ldds, gs, sizeof(double) * n, sizeof(double) * n, n,
+                              cudaMemcpyDeviceToHost, k.s), "D2H dS");
+  }
+  if (w_out) k.d2h(w_out, dw, sizeof(double) * n, "D2H w");
+  if (c_out && k.ok()) {
+    k.check(cudaMemcpy2DAsync(c_out, sizeof(double) * ldc, dc, sizeof(double) * n, sizeof(double) * n, n,
+                              cudaMemcpyDeviceToHost, k.s), "D2H C");
+  }
+  DeviceStatus st{};
+  const int code = k.finish(&st);
+  return info_of(code, st, n);
+}
+
+int xtb_gpu_set_option(const char* name, long value) {
+  if (!name) return -1;
+  if (!std::strcmp(name, "sytrd_grid")) { g_sytrd_grid = value; return 0; }
+  if (!std::strcmp(name, "ormtr_nb")) { g_ormtr_nb = value; return 0; }
+  if (!std::strcmp(name, "wait_limit_ms")) { g_wait_ms = value; return 0; }
+  return -1;
+}
+
+long xtb_gpu_get_option(const char* name) {
+  if (!name) return -1;
+  if (!std::strcmp(name, "sytrd_grid")) return g_sytrd_grid;
+  if (!std::strcmp(name, "ormtr_nb")) return g_ormtr_nb;
+  if (!std::strcmp(name, "wait_limit_ms")) return g_wait_ms;
+  return -1;
+}
+
+int xtb_gpu_last_status(void) { return t_state.last_code; }
+
+const char* xtb_gpu_last_error(void) { return t_state.last_msg.c_str(); }
+
+const char* xtb_gpu_version(void) { return "xtbeig-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,265 @@
+// Grouped GEMM kernel (see gemm.cuh).  64 x 64 output tile per CTA, 4 warps each owning 32 x 32, K in steps of 16
+// staged through shared memory by cp.async (two stages).  For FP64 every warp issues mma.sync.m8n8k4 f64: per
+// k-step of 4 a thread loads one A and one B element per 8 x 8 sub-tile (layout of the PTX ISA's m8n8k4 .f64 shape:
+// A row = lane/4, col = lane%4; B row = lane%4, col = lane/4; C row = lane/4, cols 2*(lane%4) + {0,1}).
+#include "gemm.cuh"
+
+#include "kernels.h"
+
+namespace xtbeig {
+
+namespace {
+
+constexpr int BM = kGemmBM, BN = kGemmBN, BK = kGemmBK;
+constexpr int SA = BM + 4;  // smem row stride (elements): 68 = 4 (mod 16) keeps each half-warp's fragment loads
+constexpr int SB = BN + 4;  //   on 16 distinct 8-byte banks
+
+__device__ __forceinline__ void cp_async_8(void* smem, const void* gmem, bool pred) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int sz = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_4(void* smem, const void* gmem, bool pred) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int sz = pred ? 4 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(s), "l"(gmem), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <typename T>
+__device__ __forceinline__ void cp_elem(T* smem, const T* gmem, bool pred);
+template <>
+__device__ __forceinline__ void cp_elem<double>(double* smem, const double* gmem, bool pred) {
+  cp_async_8(smem, gmem, pred);
+}
+template <>
+__device__ __forceinline__ void cp_elem<float>(float* smem, const float* gmem, bool pred) {
+  cp_async_4(smem, gmem, pred);
+}
+
+// A masked element that is not loaded must still be zero in shared memory: cp.async with src-size 0 zero-fills.
+template <typename T>
+__device__ __forceinline__ void load_tiles(const GemmDesc<T>& p, T* As, T* Bs, int m0, int n0, int k0) {
+  const int tid = threadIdx.x;
+  const int M = p.M, N = p.N, K = p.K, mode = p.mode;
+#pragma unroll
+  for (int i = 0; i < (BM * BK) / kGemmThreads; ++i) {
+    int e = tid + i * kGemmThreads;
+    int m, k;
+    if (!p.transA) { m = e % BM; k = e / BM; } else { k = e % BK; m = e / BK; }
+    int gm = m0 + m, gk = k0 + k;
+    bool ok = gm < M && gk < K;
+    if (mode & kTriAUpper) ok = ok && gk >= gm;
+    if (mode & kTriALower) ok = ok && gk <= gm;
+    const T* src = p.A;
+    if (ok) src = p.transA ? p.A + gk + (size_t)gm * p.lda : p.A + gm + (size_t)gk * p.lda;
+    cp_elem<T>(As + k * SA + m, src, ok);
+  }
+#pragma unroll
+  for (int i = 0; i < (BN * BK) / kGemmThreads; ++i) {
+    int e = tid + i * kGemmThreads;
+    int n, k;
+    if (!p.transB) { k = e % BK; n = e / BK; } else { n = e % BN; k = e / BN; }
+    int gn = n0 + n, gk = k0 + k;
+    bool ok = gn < N && gk < K;
+    if (mode & kTriBUpper) ok = ok && gk <= gn;
+    if (mode & kTriBLower) ok = ok && gk >= gn;
+    const T* src = p.B;
+    if (ok) src = p.transB ? p.B + gn + (size_t)gk * p.ldb : p.B + gk + (size_t)gn * p.ldb;
+    cp_elem<T>(Bs + k * SB + n, src, ok);
+  }
+}
+
+__device__ __forceinline__ void mma_f64(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+template <typename T>
+struct Frag;
+
+template <>
+struct Frag<double> {
+  __device__ __forceinline__ static void step(double (&acc)[4][4][2], const double* As, const double* Bs, int kk,
+                                              int wm, int wn, int lane) {
+    double a[4], b[4];
+    const int kr = kk * 4 + (lane & 3), g = lane >> 2;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = As[kr * SA + wm * 32 + i * 8 + g];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) b[j] = Bs[kr * SB + wn * 32 + j * 8 + g];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) mma_f64(acc[i][j], a[i], b[j]);
+  }
+};
+
+template <>
+struct Frag<float> {
+  __device__ __forceinline__ static void step(float (&acc)[4][4][2], const float* As, const float* Bs, int kk,
+                                              int wm, int wn, int lane) {
+    const int g = lane >> 2, c2 = (lane & 3) * 2;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int kr = kk * 4 + q;
+      float a[4], b0[4], b1[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kr * SA + wm * 32 + i * 8 + g];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        b0[j] = Bs[kr * SB + wn * 32 + j * 8 + c2];
+        b1[j] = Bs[kr * SB + wn * 32 + j * 8 + c2 + 1];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[i][j][0] = fmaf(a[i], b0[j], acc[i][j][0]);
+          acc[i][j][1] = fmaf(a[i], b1[j], acc[i][j][1]);
+        }
+    }
+  }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kGemmThreads) gemm_grouped_kernel(const GemmDesc<T>* __restrict__ descs,
+                                                                     int nprob) {
+  __shared__ __align__(16) T As[2][BK * SA];
+  __shared__ __align__(16) T Bs[2][BK * SB];
+  __shared__ int s_prob;
+
+  const int tile = blockIdx.x;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {  // last problem whose tile_begin <= tile
+      int mid = (lo + hi + 1) >> 1;
+      if (descs[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+    }
+    s_prob = lo;
+  }
+  __syncthreads();
+  const GemmDesc<T> p = descs[s_prob];
+  const int local = tile - p.tile_begin;
+  if (local < 0 || local >= p.tiles_m * p.tiles_n) return;
+  const int tm = local % p.tiles_m, tn = local / p.tiles_m;
+  const int m0 = tm * BM, n0 = tn * BN;
+  if (m0 >= p.M || n0 >= p.N) return;
+  if ((p.mode & kCUpper) && m0 > n0 + BN - 1) return;
+
+  // K range of this tile.
+  int klo = 0, khi = p.K;
+  if (p.mode & kTriAUpper) klo = max(klo, m0);
+  if (p.mode & kTriBLower) klo = max(klo, n0);
+  if (p.mode & kTriALower) khi = min(khi, m0 + BM);
+  if (p.mode & kTriBUpper) khi = min(khi, n0 + BN);
+  klo = (klo / BK) * BK;
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+  T acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = T(0);
+
+  const int nk = khi > klo ? (khi - klo + BK - 1) / BK : 0;
+  if (nk > 0) {
+    load_tiles<T>(p, As[0], Bs[0], m0, n0, klo);
+    cp_async_commit();
+    for (int it = 0; it < nk; ++it) {
+      const int cur = it & 1;
+      if (it + 1 < nk) {
+        load_tiles<T>(p, As[cur ^ 1], Bs[cur ^ 1], m0, n0, klo + (it + 1) * BK);
+        cp_async_commit();
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();
+#pragma unroll
+      for (int kk = 0; kk < BK / 4; ++kk) Frag<T>::step(acc, As[cur], Bs[cur], kk, wm, wn, lane);
+      __syncthreads();
+    }
+  }
+
+  // Epilogue.
+  const T alpha = p.alpha, beta = p.beta;
+  const int g = lane >> 2, c2 = (lane & 3) * 2;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gm = m0 + wm * 32 + i * 8 + g;
+    if (gm >= p.M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int gn = n0 + wn * 32 + j * 8 + c2 + c;
+        if (gn >= p.N) continue;
+        T* dst = p.C + gm + (size_t)gn * p.ldc;
+        T v = alpha * acc[i][j][c];
+        if (beta != T(0)) v += beta * *dst;
+        *dst = v;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void gemm_grouped_launch(const GemmDesc<T>* d_descs, int nprob, int total_tiles, cudaStream_t s) {
+  if (nprob <= 0 || total_tiles <= 0) return;
+  gemm_grouped_kernel<T><<<total_tiles, kGemmThreads, 0, s>>>(d_descs, nprob);
+}
+
+template void gemm_grouped_launch<double>(const GemmDesc<double>*, int, int, cudaStream_t);
+template void gemm_grouped_launch<float>(const GemmDesc<float>*, int, int, cudaStream_t);
+
+template <typename T>
+GemmDesc<T> gemm_problem(int M, int N, int K, T alpha, const T* A, int lda, int transA, const T* B, int ldb,
+                         int transB, T beta, T* C, int ldc, int mode) {
+  GemmDesc<T> p{};
+  p.A = A; p.B = B; p.C = C;
+  p.M = M; p.N = N; p.K = K;
+  p.lda = lda; p.ldb = ldb; p.ldc = ldc;
+  p.alpha = alpha; p.beta = beta;
+  p.transA = transA; p.transB = transB;
+  p.mode = mode;
+  return p;
+}
+
+template <typename T>
+cudaError_t gemm_group(DescArena& arena, const GemmDesc<T>* probs, int nprob, cudaStream_t s) {
+  if (nprob <= 0) return cudaSuccess;
+  char* h;
+  char* d;
+  if (!arena.take((size_t)nprob * sizeof(GemmDesc<T>), &h, &d)) return cudaErrorMemoryAllocation;
+  GemmDesc<T>* hd = reinterpret_cast<GemmDesc<T>*>(h);
+  int tb = 0;
+  for (int i = 0; i < nprob; ++i) {
+    hd[i] = probs[i];
+    const bool empty = probs[i].M <= 0 || probs[i].N <= 0;
+    hd[i].tiles_m = empty ? 0 : (probs[i].M + kGemmBM - 1) / kGemmBM;
+    hd[i].tiles_n = empty ? 0 : (probs[i].N + kGemmBN - 1) / kGemmBN;
+    hd[i].tile_begin = tb;
+    tb += hd[i].tiles_m * hd[i].tiles_n;
+  }
+  if (tb == 0) return cudaSuccess;
+  cudaError_t err = cudaMemcpyAsync(d, h, (size_t)nprob * sizeof(GemmDesc<T>), cudaMemcpyHostToDevice, s);
+  if (err != cudaSuccess) return err;
+  gemm_grouped_launch<T>(reinterpret_cast<GemmDesc<T>*>(d), nprob, tb, s);
+  return cudaGetLastError();
+}
+
+template GemmDesc<double> gemm_problem<double>(int, int, int, double, const double*, int, int, const double*, int,
+                                               int, double, double*, int, int);
+template GemmDesc<float> gemm_problem<float>(int, int, int, float, const float*, int, int, const float*, int, int,
+                                             float, float*, int, int);
+template cudaError_t gemm_group<double>(DescArena&, const GemmDesc<double>*, int, cudaStream_t);
+template cudaError_t gemm_group<float>(DescArena&, const GemmDesc<float>*, int, cudaStream_t);
+
+}  // namespace xtbeig

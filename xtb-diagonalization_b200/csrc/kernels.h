@@ -1,0 +1,135 @@
+// Internal kernel interfaces of the library (host-callable launchers).  Not part of the public C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "gemm.cuh"
+
+namespace xtbeig {
+
+// ---------------------------------------------------------------------------------------------------- sytrd
+template <typename T>
+struct SytrdParams {
+  int n;
+  const T* afull;  // full symmetric input (device), leading dimension ldf
+  int ldf;
+  T* aout;         // LAPACK-layout output (device): reflectors above the superdiagonal, e, d; ld = lda
+  int lda;
+  T* d;
+  T* e;
+  T* tau;
+  T* ybuf;         // 2 n exchange (y = A v)
+  T* cbuf;         // 2 n exchange (next column)
+  T* grows;        // global row slab when rows do not fit shared memory (grid * rows_per_cta * ldr)
+  unsigned* counter;
+  DeviceStatus* st;
+  int rows_per_cta;
+  int ldr;
+  int use_smem;
+  uint64_t limit_ns;
+};
+
+struct SytrdPlan {
+  int grid, threads, cpt, rows_per_cta, ldr;
+  bool rows_in_smem, supported;
+  size_t smem;
+};
+
+template <typename T>
+SytrdPlan sytrd_plan(int n, int num_sms, size_t max_smem, int grid_override);
+template <typename T>
+cudaError_t sytrd_launch(const SytrdParams<T>& p, const SytrdPlan& pl, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- utilities
+// dst(0:n,0:n) = symmetric matrix whose upper triangle is src's (src's strict lower triangle is not read).
+template <typename T>
+void symmetrize_upper(int n, const T* src, int lds, T* dst, int ldd, cudaStream_t s);
+// dst(0:n,0:n) = symmetric matrix whose lower triangle is src's.
+template <typename T>
+void symmetrize_lower(int n, const T* src, int lds, T* dst, int ldd, cudaStream_t s);
+// dst(j,i) = src(i,j) for i <= j: the transpose of src's upper triangle into dst's lower triangle.
+template <typename T>
+void upper_transpose_to_lower(int n, const T* src, int lds, T* dst, int ldd, cudaStream_t s);
+// Copy the upper triangle (incl. diagonal) of src into the lower triangle of the same matrix (in place).
+template <typename T>
+void mirror_upper_inplace(int n, T* a, int lda, cudaStream_t s);
+// B = A (m x n), column-major with leading dimensions.
+template <typename T>
+void copy_matrix(int m, int n, const T* a, int lda, T* b, int ldb, cudaStream_t s);
+template <typename T>
+void set_identity(int n, T* a, int lda, cudaStream_t s);
+template <typename T>
+void zero_strict_lower(int n, T* a, int lda, cudaStream_t s);
+void convert_f32_to_f64(size_t count, const float* src, double* dst, cudaStream_t s);
+void convert_f64_to_f32(size_t count, const double* src, float* dst, cudaStream_t s);
+// Strided 2-D conversions (m x n, column-major).
+void convert_mat_f32_to_f64(int m, int n, const float* a, int lda, double* b, int ldb, cudaStream_t s);
+void convert_mat_f64_to_f32(int m, int n, const double* a, int lda, float* b, int ldb, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- ormtr
+// Z(0:n, 0:m) <- Q Z with Q = H(n-2) ... H(0) from sytrd (upper).  Workspace layout in OrmtrWork.
+// Descriptor arena: GEMM descriptors are staged in pinned host memory and copied to device memory on the stream.
+// Regions are bump-allocated and only reused after the owning call has synchronised its stream (reset()).
+struct DescArena {
+  char* h = nullptr;
+  char* d = nullptr;
+  size_t cap = 0;
+  size_t off = 0;
+  void reset() { off = 0; }
+  bool take(size_t bytes, char** hp, char** dp) {
+    bytes = (bytes + 255) & ~size_t(255);
+    if (off + bytes > cap) return false;
+    *hp = h + off;
+    *dp = d + off;
+    off += bytes;
+    return true;
+  }
+};
+
+template <typename T>
+struct OrmtrWork {
+  T* V;   // n x (n-1) explicit reflectors, ld n
+  T* Tf;  // nblocks x nb x nb: Gram matrices, then forward T factors
+  T* Y;   // n x (n-1): per block Y_b = V_b T_b^T, ld n
+  T* W;   // nb x m
+};
+template <typename T>
+size_t ormtr_work_elems(int n, int m, int nb);
+template <typename T>
+OrmtrWork<T> ormtr_carve(T* base, int n, int m, int nb);
+template <typename T>
+cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, int ldz, int nb, OrmtrWork<T> w,
+                        DescArena& arena, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- stedc
+struct StedcWork;  // opaque, sized by stedc_work_bytes
+size_t stedc_work_bytes(int n);
+// Eigenpairs of the symmetric tridiagonal (d, e) on the device: d <- eigenvalues ascending, z (n x n, ldz) <-
+// orthonormal eigenvectors.  Returns LAPACK-style info through st (kStatusSecularNoConv).
+cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* work, size_t work_bytes,
+                         void* hstage, size_t hstage_bytes, DeviceStatus* st, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- potrf / trtri
+// In-place upper Cholesky of S (n x n, lds); status kStatusNotSPD with info = failing column (1-based).
+cudaError_t potrf_upper(int n, double* a, int lda, DeviceStatus* st, DescArena& arena, cudaStream_t s);
+// X = U^-1 (upper; strict lower part of X set to zero).  tmp: n x n scratch (ld n).
+cudaError_t trtri_upper(int n, const double* u, int ldu, double* x, int ldx, double* tmp, DescArena& arena,
+                        cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- adjoint
+// Daleckii-Krein gradient of sum(Wbar o C diag(f) C^T): dh, ds (n x n, ld n); t1..t3 n x n scratch.
+cudaError_t dk_adjoint(int n, const double* c, const double* e, double mu, double kt, const double* wbar, double* dh,
+                       double* ds, double* t1, double* t2, double* t3, DescArena& arena, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- helpers
+// Stage nprob descriptors through the arena (tile grid and tile_begin filled in from M, N) and launch one grouped GEMM.
+template <typename T>
+cudaError_t gemm_group(DescArena& arena, const GemmDesc<T>* probs, int nprob, cudaStream_t s);
+// One problem: C = alpha op(A) op(B) + beta C.
+template <typename T>
+GemmDesc<T> gemm_problem(int M, int N, int K, T alpha, const T* A, int lda, int transA, const T* B, int ldb,
+                         int transB, T beta, T* C, int ldc, int mode = 0);
+
+}  // namespace xtbeig

@@ -1,0 +1,151 @@
+// Back-transformation z <- Q z after the one-stage reduction: LAPACK xormtr('L', 'U', 'N') semantics, the contract of
+// xtb_dormtr_upper / xtb_sormtr_upper (reference Sources/Diagonalization/Exports.swift:56-75).  The reference applies
+// blocks of 32 reflectors in increasing order, each by three GEMMs with an explicit V^T and a larft('B') factor
+// (TridiagonalBackTransformation.swift:18-45).
+//
+// B200 design.  Reflector j (0-based, j = 0 .. n-2) is v_j = [A(0:j-1, j+1); 1; 0], tau_j, and
+// Q = H(n-2) ... H(0), so H(0) is applied first.  Blocks of nb consecutive reflectors are combined into compact WY
+// form once, all blocks in parallel:
+//   V   explicit reflector matrix (n x (n-1)),
+//   G_b = V_b^T V_b                     (grouped GEMM, all blocks in one launch),
+//   T_b forward factor from G_b         (H_j0 ... H_j1 = I - V_b T_b V_b^T; one CTA per block),
+//   Y_b = V_b T_b^T                     (grouped GEMM), since H_j1 ... H_j0 = I - V_b T_b^T V_b^T;
+// then each block is two tensor-core GEMMs on the rows it touches (0 .. j0 + nb - 1):
+//   W = V_b^T Z,   Z -= Y_b W.
+// Larger blocks than the reference's 32 cut the number of passes over Z (n/nb sweeps of an n x m matrix); the extra
+// flops of the explicit Y are n^2 nb per block.
+#include <algorithm>
+
+#include "kernels.h"
+
+namespace xtbeig {
+
+namespace {
+
+template <typename T>
+__global__ void build_v_kernel(int n, const T* __restrict__ a, int lda, T* __restrict__ v) {
+  const size_t total = (size_t)n * (n - 1);
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx % n), j = (int)(idx / n);
+    T val;
+    if (r < j) val = a[r + (size_t)(j + 1) * lda];
+    else val = (r == j) ? T(1) : T(0);
+    v[idx] = val;
+  }
+}
+
+// In place: Tf_b holds G_b = V_b^T V_b (kb x kb, ld nb) on entry and the upper-triangular forward factor T_b on exit:
+// T(i,i) = tau_i, T(0:i-1, i) = -tau_i T(0:i-1, 0:i-1) G(0:i-1, i).  The factor is built in shared memory.
+template <typename T>
+__global__ void wy_factor_kernel(int nm1, int nb, const T* __restrict__ tau, T* __restrict__ tf) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Ts = reinterpret_cast<T*>(smem_raw);  // nb x nb, ld nb
+  T* g = Ts + (size_t)nb * nb;             // column of G
+  const int b = blockIdx.x;
+  const int j0 = b * nb;
+  const int kb = min(nb, nm1 - j0);
+  T* tb = tf + (size_t)b * nb * nb;
+  for (int i = 0; i < kb; ++i) {
+    for (int r = threadIdx.x; r < i; r += blockDim.x) g[r] = tb[r + (size_t)i * nb];
+    __syncthreads();
+    const T ti = tau[j0 + i];
+    for (int r = threadIdx.x; r < kb; r += blockDim.x) {
+      T val;
+      if (r < i) {
+        T acc = T(0);
+        for (int c = r; c < i; ++c) acc += Ts[r + (size_t)c * nb] * g[c];
+        val = -ti * acc;
+      } else {
+        val = (r == i) ? ti : T(0);
+      }
+      Ts[r + (size_t)i * nb] = val;
+    }
+    __syncthreads();
+  }
+  for (size_t idx = threadIdx.x; idx < (size_t)kb * kb; idx += blockDim.x) {
+    const int r = (int)(idx % kb), c = (int)(idx / kb);
+    tb[r + (size_t)c * nb] = Ts[r + (size_t)c * nb];
+  }
+}
+
+}  // namespace
+
+template <typename T>
+size_t ormtr_work_elems(int n, int m, int nb) {
+  const size_t nm1 = n > 1 ? (size_t)(n - 1) : 1;
+  const size_t nblocks = (nm1 + nb - 1) / nb;
+  return 2 * (size_t)n * nm1 + nblocks * nb * nb + (size_t)nb * (m > 0 ? m : 1) + 4 * 64;
+}
+
+template <typename T>
+OrmtrWork<T> ormtr_carve(T* base, int n, int m, int nb) {
+  const size_t nm1 = n > 1 ? (size_t)(n - 1) : 1;
+  const size_t nblocks = (nm1 + nb - 1) / nb;
+  auto up = [](size_t e) { return (e + 63) & ~size_t(63); };
+  OrmtrWork<T> w;
+  T* p = base;
+  w.V = p; p += up((size_t)n * nm1);
+  w.Y = p; p += up((size_t)n * nm1);
+  w.Tf = p; p += up(nblocks * nb * nb);
+  w.W = p;
+  return w;
+}
+
+template <typename T>
+cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, int ldz, int nb, OrmtrWork<T> w,
+                        DescArena& arena, cudaStream_t s) {
+  if (n <= 1 || m <= 0) return cudaSuccess;
+  const int nm1 = n - 1;
+  const int nblocks = (nm1 + nb - 1) / nb;
+  {
+    const size_t total = (size_t)n * nm1;
+    int grid = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+    build_v_kernel<T><<<grid, 256, 0, s>>>(n, a, lda, w.V);
+  }
+  // Gram matrices of all blocks, one grouped launch.
+  GemmDesc<T>* probs = new GemmDesc<T>[nblocks];
+  for (int b = 0; b < nblocks; ++b) {
+    const int j0 = b * nb, kb = std::min(nb, nm1 - j0), rows = j0 + kb;
+    const T* vb = w.V + (size_t)j0 * n;
+    probs[b] = gemm_problem<T>(kb, kb, rows, T(1), vb, n, 1, vb, n, 0, T(0), w.Tf + (size_t)b * nb * nb, nb);
+  }
+  cudaError_t err = gemm_group<T>(arena, probs, nblocks, s);
+  if (err != cudaSuccess) { delete[] probs; return err; }
+  {
+    const size_t smem = ((size_t)nb * nb + nb) * sizeof(T);
+    err = cudaFuncSetAttribute(wy_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) { delete[] probs; return err; }
+    wy_factor_kernel<T><<<nblocks, 128, smem, s>>>(nm1, nb, tau, w.Tf);
+  }
+  // Y_b = V_b T_b^T (op(B) = T_b^T is lower triangular).
+  for (int b = 0; b < nblocks; ++b) {
+    const int j0 = b * nb, kb = std::min(nb, nm1 - j0), rows = j0 + kb;
+    probs[b] = gemm_problem<T>(rows, kb, kb, T(1), w.V + (size_t)j0 * n, n, 0, w.Tf + (size_t)b * nb * nb, nb, 1,
+                               T(0), w.Y + (size_t)j0 * n, n, kTriBLower);
+  }
+  err = gemm_group<T>(arena, probs, nblocks, s);
+  delete[] probs;
+  if (err != cudaSuccess) return err;
+  // Apply the blocks in increasing order.
+  for (int b = 0; b < nblocks; ++b) {
+    const int j0 = b * nb, kb = std::min(nb, nm1 - j0), rows = j0 + kb;
+    GemmDesc<T> p1 = gemm_problem<T>(kb, m, rows, T(1), w.V + (size_t)j0 * n, n, 1, z, ldz, 0, T(0), w.W, nb);
+    err = gemm_group<T>(arena, &p1, 1, s);
+    if (err != cudaSuccess) return err;
+    GemmDesc<T> p2 = gemm_problem<T>(rows, m, kb, T(-1), w.Y + (size_t)j0 * n, n, 0, w.W, nb, 0, T(1), z, ldz);
+    err = gemm_group<T>(arena, &p2, 1, s);
+    if (err != cudaSuccess) return err;
+  }
+  return cudaGetLastError();
+}
+
+template size_t ormtr_work_elems<double>(int, int, int);
+template size_t ormtr_work_elems<float>(int, int, int);
+template OrmtrWork<double> ormtr_carve<double>(double*, int, int, int);
+template OrmtrWork<float> ormtr_carve<float>(float*, int, int, int);
+template cudaError_t ormtr_upper<double>(int, int, const double*, int, const double*, double*, int, int,
+                                         OrmtrWork<double>, DescArena&, cudaStream_t);
+template cudaError_t ormtr_upper<float>(int, int, const float*, int, const float*, float*, int, int,
+                                        OrmtrWork<float>, DescArena&, cudaStream_t);
+
+}  // namespace xtbeig

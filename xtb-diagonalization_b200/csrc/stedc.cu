@@ -1,0 +1,751 @@
+// Divide and conquer for the symmetric tridiagonal eigenproblem on the device (the contract of LAPACK xstedc with
+// COMPZ = 'I', which xtb_dstedc exposes: reference Sources/Diagonalization/Exports.swift:88-115; the reference's own
+// merge is Stages/ParallelDivideAndConquer.swift:42-211, a port of LAPACK's dlaed1/2/3).
+//
+// B200 design.  The recursion is flattened into levels: the tree of tears is fixed by n alone, so every merge of one
+// level runs in the same launches (one CTA or warp per merge / root / column), bottom-up from 1 x 1 leaves.  Per level:
+//   deflate   one CTA per merge: z from the halves' boundary rows, merge-sort of the two ascending eigenvalue lists,
+//             small-z deflation (rho |z_i| <= tol) and close-pair deflation by Givens rotation (Dongarra-Sorensen),
+//             classification of the surviving columns (upper half only / both / lower half only) so the merge GEMM
+//             skips the zero blocks, and the device-side sizes of the two merge GEMMs;
+//   rotate    apply the recorded rotations to the eigenvector columns, gather survivors and deflated columns;
+//   secular   one warp per root, FP64: lambda_j = dlamda_o + tau with tau relative to the nearer pole (so that
+//             dlamda_i - lambda_j is formed without cancellation), iterated with the two-pole rational model of the
+//             secular function ("middle way", R.-C. Li 1993) inside a bisection bracket;
+//   zhat      one warp per i: Gu and Eisenstat's recomputed z (1995) from the computed roots, which makes the
+//             eigenvectors of the rank-one problem numerically orthogonal;
+//   vectors   one warp per column: u_j = zhat ./ (dlamda - lambda_j), normalised, rows placed in GEMM order;
+//   gemm      two grouped FP64 tensor-core GEMMs per merge (upper rows, lower rows);
+//   order     final ascending order of roots and deflated eigenvalues, columns copied into place.
+// The tridiagonal is scaled by max(|d|, |e|) first and the eigenvalues scaled back, as xstedc does.  No floating-point
+// atomics are used, so results are deterministic.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace xtbeig {
+
+namespace {
+
+struct MergeDesc {
+  int s, n1, n2, pad;
+};
+
+struct MergeInfo {
+  int K;       // surviving (non-deflated) count
+  int c1, c2, c3;
+  int nrot;
+  int ndefl;
+  double rho;
+};
+
+struct DcBufs {
+  int n;       // total size
+  int ld;      // leading dimension of the n x n work matrices (= n)
+  double* dd;  // current eigenvalues by position
+  double* ee;  // scaled off-diagonal
+  double* Qa;  // eigenvectors (input of the level)
+  double* Qb;  // eigenvectors (output of the level)
+  double* Qc;  // gathered columns: survivors in GEMM order, then deflated
+  double* Up;  // rank-one eigenvectors, rows in GEMM order
+  double* Dl;  // dlamda_i - lambda_j
+  double* sd;  // sorted d (then updated by deflation)
+  double* sz;  // sorted z
+  double* dlam;  // survivors' poles
+  double* zk;    // survivors' z
+  double* zh;    // recomputed z
+  double* lam;   // roots
+  double* dval;  // deflated eigenvalues (position order)
+  double* rotc;
+  double* rots;
+  double* scale;  // [1] max norm of (d, e)
+  int* sperm;     // sorted position -> local column
+  int* typ;       // column type by sorted position (1: upper only, 2: both, 3: lower only, 4: deflated)
+  int* ndl;       // scratch list of non-deflated positions
+  int* cand;      // pair candidate flags
+  int* slotOf;    // survivor index -> GEMM slot
+  int* srcCol;    // Qc column -> local source column in Qa
+  int* outSrc;    // output position -> source (j < K: root j; K + t: deflated t)
+  int* rotI;
+  int* rotJ;
+  int* posMerge;  // global position -> merge index at the current level
+  MergeDesc* merges;
+  MergeInfo* info;
+  GemmDesc<double>* gdesc;  // 2 per merge
+  DeviceStatus* st;
+};
+
+constexpr double kEps = 1.1102230246251565e-16;
+
+// ------------------------------------------------------------------------------------------------ set-up kernels
+
+__global__ void dc_scale_kernel(int n, const double* d, const double* e, double* scale) {
+  __shared__ double scratch[32];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, fabs(d[i]));
+  for (int i = threadIdx.x; i < n - 1; i += blockDim.x) m = fmax(m, fabs(e[i]));
+  m = block_max(m, scratch);
+  if (threadIdx.x == 0) scale[0] = m;
+}
+
+// dd = d / scale with every split point torn (LAPACK dlaed0's tear: both neighbours lose |e|), ee = e / scale.
+__global__ void dc_init_kernel(int n, const double* d, const double* e, double* dd, double* ee,
+                               const double* scale) {
+  const double sc = scale[0];
+  const double inv = sc > 0.0 ? 1.0 / sc : 1.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v = d[i] * inv;
+    if (i > 0) v -= fabs(e[i - 1] * inv);
+    if (i < n - 1) v -= fabs(e[i] * inv);
+    dd[i] = v;
+    if (i < n - 1) ee[i] = e[i] * inv;
+  }
+}
+
+// Both ping-pong buffers start as the identity and both eigenvalue buffers as the torn diagonal: a 1 x 1 leaf that no
+// merge of the current level covers then reads its initial state from whichever buffer is current.
+__global__ void dc_identity_kernel(int n, int ld, double* q, double* qb, const double* dd, double* dnext) {
+  size_t total = (size_t)n * n;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(idx % n), j = (int)(idx / n);
+    const double v = (i == j) ? 1.0 : 0.0;
+    q[i + (size_t)j * ld] = v;
+    qb[i + (size_t)j * ld] = v;
+    if (j == 0) dnext[i] = dd[i];
+  }
+}
+
+// Block-wide exclusive scan of one int per thread; returns the exclusive prefix, *total receives the sum.
+__device__ int block_exscan(int v, int* scratch, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  __syncthreads();
+  if (lane == 31) scratch[warp] = x;
+  __syncthreads();
+  int wpre = 0, tot = 0;
+  for (int w = 0; w < nw; ++w) {
+    if (w < warp) wpre += scratch[w];
+    tot += scratch[w];
+  }
+  *total = tot;
+  return wpre + x - v;
+}
+
+// ------------------------------------------------------------------------------------------------ deflate
+
+__global__ void __launch_bounds__(1024) dc_deflate_kernel(DcBufs B, int nmerge) {
+  __shared__ double s_red[32];
+  __shared__ int s_scan[32];
+  __shared__ int s_cnt[8];
+  const int mi = blockIdx.x;
+  if (mi >= nmerge) return;
+  const MergeDesc md = B.merges[mi];
+  const int s = md.s, n1 = md.n1, n2 = md.n2, n = n1 + n2;
+  const size_t ld = B.ld;
+  const double beta = B.ee[s + n1 - 1];
+  const double rho = 2.0 * fabs(beta);
+  const double sgn = beta >= 0.0 ? 1.0 : -1.0;
+  const double rs2 = 0.70710678118654752440;
+  const double* dd = B.dd + s;
+  double* sd = B.sd + s;
+  double* sz = B.sz + s;
+  int* sperm = B.sperm + s;
+  int* typ = B.typ + s;
+
+  // z and the merge of the two ascending lists (stable: ties keep the upper half first).
+  double dmax = 0.0, zmax = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double dv, zv;
+    int rank;
+    if (i < n1) {
+      dv = dd[i];
+      zv = B.Qa[(size_t)(s + n1 - 1) + (size_t)(s + i) * ld] * rs2;
+      int lo = 0, hi = n2;  // count second-half values < dv
+      while (lo < hi) { int m = (lo + hi) >> 1; if (dd[n1 + m] < dv) lo = m + 1; else hi = m; }
+      rank = i + lo;
+    } else {
+      const int j = i - n1;
+      dv = dd[i];
+      zv = sgn * B.Qa[(size_t)(s + n1) + (size_t)(s + i) * ld] * rs2;
+      int lo = 0, hi = n1;  // count first-half values <= dv
+      while (lo < hi) { int m = (lo + hi) >> 1; if (dd[m] <= dv) lo = m + 1; else hi = m; }
+      rank = j + lo;
+    }
+    sd[rank] = dv;
+    sz[rank] = zv;
+    sperm[rank] = i;
+    typ[rank] = i < n1 ? 1 : 3;
+    dmax = fmax(dmax, fabs(dv));
+    zmax = fmax(zmax, fabs(zv));
+  }
+  dmax = block_max(dmax, s_red);
+  zmax = block_max(zmax, s_red);
+  const double tol = 8.0 * kEps * fmax(dmax, zmax);
+  __syncthreads();
+
+  // Small-z deflation, then the compacted list of candidates for pair deflation.
+  int* ndl = B.ndl + s;
+  int* cand = B.cand + s;
+  int m = 0;
+  for (int base = 0; base < n; base += blockDim.x) {
+    const int p = base + threadIdx.x;
+    int keep = 0;
+    if (p < n) {
+      keep = rho * fabs(sz[p]) > tol;
+      if (!keep) typ[p] = 4;
+    }
+    int tot;
+    int pre = block_exscan(keep, s_scan, &tot);
+    if (keep) ndl[m + pre] = p;
+    m += tot;
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < m - 1; i += blockDim.x) {
+    const int a = ndl[i], b = ndl[i + 1];
+    const double za = sz[a], zb = sz[b];
+    const double t = hypot(za, zb);
+    const double c = zb / t, sn = -za / t;
+    cand[i] = fabs((sd[b] - sd[a]) * c * sn) <= tol;
+  }
+  __syncthreads();
+
+  // Sequential chain of close-pair deflations (rare; the test of pair i uses the survivor of pair i-1).
+  if (threadIdx.x == 0) {
+    int nrot = 0;
+    bool modified = false;
+    for (int i = 0; i < m - 1; ++i) {
+      if (!cand[i] && !modified) continue;
+      const int a = ndl[i], b = ndl[i + 1];
+      const double za = sz[a], zb = sz[b];
+      const double t = hypot(za, zb);
+      const double c = zb / t, sn = -za / t;
+      const double da = sd[a], db = sd[b];
+      if (fabs((db - da) * c * sn) <= tol) {
+        sz[b] = t;
+        sz[a] = 0.0;
+        sd[a] = da * c * c + db * sn * sn;
+        sd[b] = da * sn * sn + db * c * c;
+        if (typ[a] != typ[b]) typ[b] = 2;
+        typ[a] = 4;
+        B.rotI[s + nrot] = sperm[a];
+        B.rotJ[s + nrot] = sperm[b];
+        B.rotc[s + nrot] = c;
+        B.rots[s + nrot] = sn;
+        ++nrot;
+        modified = true;
+      } else {
+        modified = false;
+      }
+    }
+    s_cnt[0] = nrot;
+  }
+  __syncthreads();
+
+  // Survivors in position order (their values ascend), their type-grouped GEMM slots, deflated list.
+  // Pass 1: counts per type.
+  int cnt[4] = {0, 0, 0, 0};
+  for (int p = threadIdx.x; p < n; p += blockDim.x) cnt[typ[p] - 1]++;
+  for (int t = 0; t < 4; ++t) {
+    int tot;
+    (void)block_exscan(cnt[t], s_scan, &tot);
+    if (threadIdx.x == 0) s_cnt[1 + t] = tot;
+    __syncthreads();
+  }
+  const int c1 = s_cnt[1], c2 = s_cnt[2], c3 = s_cnt[3], nd = s_cnt[4];
+  const int K = c1 + c2 + c3;
+  // Pass 2: ordered ranks (survivor index i, per-type rank, deflated rank).
+  int run_i = 0, run_t[3] = {0, 0, 0}, run_d = 0;
+  for (int base = 0; base < n; base += blockDim.x) {
+    const int p = base + threadIdx.x;
+    const int ty = p < n ? typ[p] : 0;
+    const int isS = (ty >= 1 && ty <= 3), isD = (ty == 4);
+    int tot_s, tot_d, tot_t[3];
+    const int pre_s = block_exscan(isS, s_scan, &tot_s);
+    __syncthreads();
+    const int pre_d = block_exscan(isD, s_scan, &tot_d);
+    int pre_t[3];
+    for (int t = 0; t < 3; ++t) {
+      __syncthreads();
+      pre_t[t] = block_exscan(ty == t + 1, s_scan, &tot_t[t]);
+    }
+    if (isS) {
+      const int i = run_i + pre_s;
+      int slot;
+      if (ty == 1) slot = run_t[0] + pre_t[0];
+      else if (ty == 2) slot = c1 + run_t[1] + pre_t[1];
+      else slot = c1 + c2 + run_t[2] + pre_t[2];
+      B.dlam[s + i] = sd[p];
+      B.zk[s + i] = sz[p];
+      B.slotOf[s + i] = slot;
+      B.srcCol[s + slot] = sperm[p];
+    } else if (isD) {
+      const int t = run_d + pre_d;
+      B.dval[s + t] = sd[p];
+      B.srcCol[s + K + t] = sperm[p];
+    }
+    run_i += tot_s;
+    run_d += tot_d;
+    for (int t = 0; t < 3; ++t) run_t[t] += tot_t[t];
+    __syncthreads();
+  }
+
+  if (threadIdx.x == 0) {
+    MergeInfo inf;
+    inf.K = K; inf.c1 = c1; inf.c2 = c2; inf.c3 = c3; inf.nrot = s_cnt[0]; inf.ndefl = nd; inf.rho = rho;
+    B.info[mi] = inf;
+    // Merge GEMMs: Qnew(upper rows) = Qc(upper, slots [0, c1+c2)) Up(slots [0, c1+c2), 0:K);
+    //              Qnew(lower rows) = Qc(lower, slots [c1, K))     Up(slots [c1, K), 0:K).   Qnew overwrites Qa.
+    GemmDesc<double>& gt = B.gdesc[2 * mi];
+    GemmDesc<double>& gb = B.gdesc[2 * mi + 1];
+    gt.A = B.Qc + (size_t)s + (size_t)s * ld;
+    gt.B = B.Up + (size_t)s + (size_t)s * ld;
+    gt.C = B.Qa + (size_t)s + (size_t)s * ld;
+    gt.M = n1; gt.N = K; gt.K = c1 + c2;
+    gb.A = B.Qc + (size_t)(s + n1) + (size_t)(s + c1) * ld;
+    gb.B = B.Up + (size_t)(s + c1) + (size_t)s * ld;
+    gb.C = B.Qa + (size_t)(s + n1) + (size_t)s * ld;
+    gb.M = n2; gb.N = K; gb.K = c2 + c3;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ rotate + gather
+
+// grid (merges, row blocks); one thread per row of the merge block.
+__global__ void dc_rotate_gather_kernel(DcBufs B) {
+  const int mi = blockIdx.x;
+  const MergeDesc md = B.merges[mi];
+  const MergeInfo inf = B.info[mi];
+  const int s = md.s, n = md.n1 + md.n2;
+  const size_t ld = B.ld;
+  const int r = blockIdx.y * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double* qrow = B.Qa + (size_t)(s + r) + (size_t)s * ld;  // element (r, c) at qrow[c * ld]
+  for (int t = 0; t < inf.nrot; ++t) {
+    const int i = B.rotI[s + t], j = B.rotJ[s + t];
+    const double c = B.rotc[s + t], sn = B.rots[s + t];
+    const double qi = qrow[(size_t)i * ld], qj = qrow[(size_t)j * ld];
+    qrow[(size_t)i * ld] = c * qi + sn * qj;
+    qrow[(size_t)j * ld] = -sn * qi + c * qj;
+  }
+  double* crow = B.Qc + (size_t)(s + r) + (size_t)s * ld;
+  for (int col = 0; col < n; ++col) crow[(size_t)col * ld] = qrow[(size_t)B.srcCol[s + col] * ld];
+}
+
+// ------------------------------------------------------------------------------------------------ secular equation
+
+struct SecSums {
+  double psi, dpsi, phi, dphi, asum;
+};
+
+__device__ __forceinline__ SecSums sec_eval(const double* dl, const double* z, int K, int o, int a, double tau) {
+  const int lane = threadIdx.x & 31;
+  SecSums r{0, 0, 0, 0, 0};
+  const double dlo = dl[o];
+  for (int i = lane; i < K; i += 32) {
+    const double del = (dl[i] - dlo) - tau;
+    const double inv = 1.0 / del;
+    const double t = z[i] * z[i] * inv;
+    if (i <= a) { r.psi += t; r.dpsi += t * inv; } else { r.phi += t; r.dphi += t * inv; }
+    r.asum += fabs(t);
+  }
+  r.psi = warp_sum(r.psi);
+  r.dpsi = warp_sum(r.dpsi);
+  r.phi = warp_sum(r.phi);
+  r.dphi = warp_sum(r.dphi);
+  r.asum = warp_sum(r.asum);
+  return r;
+}
+
+// Root j of 1/rho + sum_i z_i^2 / (dl_i - lambda) = 0 (rho > 0, dl ascending): lambda = dl[o] + tau.
+// Returns false if it did not converge within the iteration limit (the best iterate is still returned).
+__device__ bool secular_root(const double* dl, const double* z, int K, double rho, int j, int* o_out,
+                             double* tau_out) {
+  const int lane = threadIdx.x & 31;
+  const double rinv = 1.0 / rho;
+  if (K == 1) {
+    *o_out = 0;
+    *tau_out = rho * z[0] * z[0];
+    return true;
+  }
+  int o, a;
+  double lo, hi;
+  if (j < K - 1) {
+    const double dj = dl[j], gap = dl[j + 1] - dj;
+    double fm = 0.0;
+    for (int i = lane; i < K; i += 32) fm += z[i] * z[i] / ((dl[i] - dj) - 0.5 * gap);
+    fm = rinv + warp_sum(fm);
+    if (fm >= 0.0) { o = j; lo = 0.0; hi = 0.5 * gap; }
+    else { o = j + 1; lo = -0.5 * gap; hi = 0.0; }
+    a = j;
+  } else {
+    double zz = 0.0;
+    for (int i = lane; i < K; i += 32) zz += z[i] * z[i];
+    zz = warp_sum(zz);
+    o = K - 1;
+    lo = 0.0;
+    hi = rho * zz;
+    a = K - 2;
+  }
+  const int b = a + 1;
+  const double dlo = dl[o];
+  const double pa = dl[a] - dlo, pb = dl[b] - dlo;  // poles relative to the origin
+  double tau = 0.5 * (lo + hi);
+  bool conv = false;
+  for (int it = 0; it < 120; ++it) {
+    const SecSums S = sec_eval(dl, z, K, o, a, tau);
+    const double f = rinv + S.psi + S.phi;
+    const double errb = 8.0 * kEps * (rinv + S.asum) + kEps * fabs(tau) * (S.dpsi + S.dphi);
+    if (fabs(f) <= errb) { conv = true; break; }
+    if (f < 0.0) lo = tau; else hi = tau;
+    if (hi - lo <= 2.0 * kEps * fmax(fabs(lo), fabs(hi))) { conv = true; break; }
+    // Two-pole rational model c + A/(da - eta) + B/(db - eta) matching psi, psi', phi, phi' at tau.
+    const double da = pa - tau, db = pb - tau;
+    const double A = S.dpsi * da * da, Bm = S.dphi * db * db;
+    const double c = f - S.dpsi * da - S.dphi * db;
+    const double bq = c * (da + db) + A + Bm, cq = da * db * f;
+    double cand1 = NAN, cand2 = NAN;
+    if (c == 0.0) {
+      if (bq != 0.0) cand1 = cq / bq;
+    } else {
+      double disc = bq * bq - 4.0 * c * cq;
+      if (disc < 0.0) disc = 0.0;
+      const double sq = sqrt(disc);
+      const double big = (bq >= 0.0) ? (bq + sq) : (bq - sq);
+      if (big != 0.0) {
+        cand1 = big / (2.0 * c);
+        cand2 = 2.0 * cq / big;
+      }
+    }
+    double tn = NAN;
+    const double e1 = tau + cand1, e2 = tau + cand2;
+    const bool ok1 = (e1 > lo) && (e1 < hi), ok2 = (e2 > lo) && (e2 < hi);
+    if (ok1 && !ok2) tn = e1;
+    else if (ok2 && !ok1) tn = e2;
+    else if (ok1 && ok2) tn = fabs(cand1) < fabs(cand2) ? e1 : e2;
+    if (!(tn > lo && tn < hi)) tn = 0.5 * (lo + hi);
+    if (tn == tau) { conv = true; break; }
+    tau = tn;
+  }
+  *o_out = o;
+  *tau_out = tau;
+  return conv;
+}
+
+// One warp per global position; position s + j of a merge with j < K solves root j.
+__global__ void dc_secular_kernel(DcBufs B) {
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= B.n) return;
+  const int mi = B.posMerge[gw];
+  if (mi < 0) return;
+  const MergeDesc md = B.merges[mi];
+  const MergeInfo inf = B.info[mi];
+  const int s = md.s, j = gw - s, K = inf.K;
+  if (j >= K) return;
+  const double* dl = B.dlam + s;
+  const double* z = B.zk + s;
+  int o;
+  double tau;
+  const bool ok = secular_root(dl, z, K, inf.rho, j, &o, &tau);
+  if (!ok && lane == 0) set_status(B.st, kStatusSecularNoConv, s + j + 1, s);
+  const size_t ld = B.ld;
+  double* col = B.Dl + (size_t)s + (size_t)(s + j) * ld;
+  const double dlo = dl[o];
+  for (int i = lane; i < K; i += 32) col[i] = (dl[i] - dlo) - tau;
+  if (lane == 0) B.lam[s + j] = dlo + tau;
+}
+
+// One warp per survivor i: zhat_i^2 = -prod_j (dl_i - lambda_j) / prod_{j != i} (dl_i - dl_j)  (Gu-Eisenstat).
+__global__ void dc_zhat_kernel(DcBufs B) {
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= B.n) return;
+  const int mi = B.posMerge[gw];
+  if (mi < 0) return;
+  const MergeDesc md = B.merges[mi];
+  const MergeInfo inf = B.info[mi];
+  const int s = md.s, i = gw - s, K = inf.K;
+  if (i >= K) return;
+  const size_t ld = B.ld;
+  const double* dl = B.dlam + s;
+  const double di = dl[i];
+  double prod = 1.0;
+  for (int j = lane; j < K; j += 32) {
+    const double del = B.Dl[(size_t)(s + i) + (size_t)(s + j) * ld];
+    prod *= (j == i) ? -del : del / (di - dl[j]);
+  }
+  prod = warp_prod(prod);
+  if (lane == 0) {
+    const double mag = sqrt(fmax(prod, 0.0));
+    B.zh[s + i] = copysign(mag, B.zk[s + i]);
+  }
+}
+
+// One warp per root j: column j of the rank-one problem's eigenvectors, rows in GEMM slot order.
+__global__ void dc_vectors_kernel(DcBufs B) {
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= B.n) return;
+  const int mi = B.posMerge[gw];
+  if (mi < 0) return;
+  const MergeDesc md = B.merges[mi];
+  const MergeInfo inf = B.info[mi];
+  const int s = md.s, j = gw - s, K = inf.K;
+  if (j >= K) return;
+  const size_t ld = B.ld;
+  double* up = B.Up + (size_t)s + (size_t)(s + j) * ld;
+  if (K == 1) {
+    if (lane == 0) up[B.slotOf[s]] = 1.0;
+    return;
+  }
+  const double* dcol = B.Dl + (size_t)s + (size_t)(s + j) * ld;
+  double ss = 0.0;
+  for (int i = lane; i < K; i += 32) {
+    const double u = B.zh[s + i] / dcol[i];
+    ss += u * u;
+  }
+  ss = warp_sum(ss);
+  const double inv = 1.0 / sqrt(ss);
+  for (int i = lane; i < K; i += 32) up[B.slotOf[s + i]] = (B.zh[s + i] / dcol[i]) * inv;
+}
+
+// ------------------------------------------------------------------------------------------------ final order
+
+// One CTA per merge: rank of every root and deflated value in the merged ascending order.
+__global__ void dc_order_kernel(DcBufs B, double* dnext) {
+  const int mi = blockIdx.x;
+  const MergeDesc md = B.merges[mi];
+  const MergeInfo inf = B.info[mi];
+  const int s = md.s, n = md.n1 + md.n2, K = inf.K, nd = n - K;
+  const double* lam = B.lam + s;
+  const double* dv = B.dval + s;
+  for (int j = threadIdx.x; j < K; j += blockDim.x) {
+    const double x = lam[j];
+    int c = 0;
+    for (int t = 0; t < nd; ++t) c += dv[t] < x;
+    const int rank = j + c;
+    B.outSrc[s + rank] = j;
+    dnext[s + rank] = x;
+  }
+  for (int t = threadIdx.x; t < nd; t += blockDim.x) {
+    const double x = dv[t];
+    int lo = 0, hi = K;  // roots <= x
+    while (lo < hi) { int m = (lo + hi) >> 1; if (lam[m] <= x) lo = m + 1; else hi = m; }
+    int c = lo;
+    for (int u = 0; u < nd; ++u) c += (dv[u] < x) || (dv[u] == x && u < t);
+    B.outSrc[s + c] = K + t;
+    dnext[s + c] = x;
+  }
+}
+
+// grid (merges, column blocks of 8): copy each output column into the next level's eigenvector matrix.
+__global__ void dc_copy_kernel(DcBufs B) {
+  const int mi = blockIdx.x;
+  const MergeDesc md = B.merges[mi];
+  const MergeInfo inf = B.info[mi];
+  const int s = md.s, n = md.n1 + md.n2, K = inf.K;
+  const size_t ld = B.ld;
+  const int c0 = blockIdx.y * 8;
+  for (int c = c0; c < min(c0 + 8, n); ++c) {
+    const int src = B.outSrc[s + c];
+    const double* from = (src < K ? B.Qa : B.Qc) + (size_t)s + (size_t)(s + src) * ld;
+    double* to = B.Qb + (size_t)s + (size_t)(s + c) * ld;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) to[r] = from[r];
+  }
+}
+
+__global__ void dc_finish_kernel(int n, const double* dd, const double* scale, double* d_out, const double* q,
+                                 int ldq, double* z, int ldz) {
+  const double sc = scale[0] > 0.0 ? scale[0] : 1.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d_out[i] = dd[i] * sc;
+  const size_t total = (size_t)n * n;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % n), j = (int)(idx / n);
+    z[i + (size_t)j * ldz] = q[i + (size_t)j * ldq];
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ host plan
+
+struct Level {
+  std::vector<MergeDesc> merges;
+};
+
+void build_levels(int s, int n, int depth, std::vector<Level>& levels) {
+  if (n <= 1) return;
+  const int n1 = n / 2, n2 = n - n1;
+  build_levels(s, n1, depth + 1, levels);
+  build_levels(s + n1, n2, depth + 1, levels);
+  if ((int)levels.size() <= depth) levels.resize(depth + 1);
+  levels[depth].merges.push_back(MergeDesc{s, n1, n2, 0});
+}
+
+template <typename T>
+T* carve(char*& p, size_t count) {
+  T* r = reinterpret_cast<T*>(p);
+  p += ((count * sizeof(T) + 255) / 256) * 256;
+  return r;
+}
+
+}  // namespace
+
+size_t stedc_work_bytes(int n) {
+  const size_t nn = (size_t)n * n;
+  size_t b = 0;
+  auto add = [&](size_t bytes) { b += ((bytes + 255) / 256) * 256; };
+  add(n * sizeof(double) * 2);         // dd, ee
+  for (int i = 0; i < 5; ++i) add(nn * sizeof(double));  // Qa Qb Qc Up Dl
+  for (int i = 0; i < 10; ++i) add(n * sizeof(double));  // sd sz dlam zk zh lam dval rotc rots dnext
+  add(sizeof(double) * 4);             // scale
+  for (int i = 0; i < 9; ++i) add(n * sizeof(int));      // sperm typ ndl cand slotOf srcCol outSrc rotI rotJ
+  // per level: posMerge, merges, info, gemm descriptors (levels <= 32)
+  add((size_t)32 * n * sizeof(int));
+  add((size_t)32 * (n / 2 + 2) * sizeof(MergeDesc));
+  add((size_t)(n / 2 + 2) * sizeof(MergeInfo));
+  add((size_t)32 * (n + 4) * sizeof(GemmDesc<double>));
+  return b;
+}
+
+cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* work, size_t work_bytes,
+                         void* hstage, size_t hstage_bytes, DeviceStatus* st, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  if (work_bytes < stedc_work_bytes(n)) return cudaErrorInvalidValue;
+  char* p = reinterpret_cast<char*>(work);
+  DcBufs B{};
+  B.n = n;
+  B.ld = n;
+  const size_t nn = (size_t)n * n;
+  B.dd = carve<double>(p, n);
+  B.ee = carve<double>(p, n);
+  B.Qa = carve<double>(p, nn);
+  B.Qb = carve<double>(p, nn);
+  B.Qc = carve<double>(p, nn);
+  B.Up = carve<double>(p, nn);
+  B.Dl = carve<double>(p, nn);
+  B.sd = carve<double>(p, n);
+  B.sz = carve<double>(p, n);
+  B.dlam = carve<double>(p, n);
+  B.zk = carve<double>(p, n);
+  B.zh = carve<double>(p, n);
+  B.lam = carve<double>(p, n);
+  B.dval = carve<double>(p, n);
+  B.rotc = carve<double>(p, n);
+  B.rots = carve<double>(p, n);
+  double* dnext = carve<double>(p, n);
+  B.scale = carve<double>(p, 4);
+  B.sperm = carve<int>(p, n);
+  B.typ = carve<int>(p, n);
+  B.ndl = carve<int>(p, n);
+  B.cand = carve<int>(p, n);
+  B.slotOf = carve<int>(p, n);
+  B.srcCol = carve<int>(p, n);
+  B.outSrc = carve<int>(p, n);
+  B.rotI = carve<int>(p, n);
+  B.rotJ = carve<int>(p, n);
+  int* posAll = carve<int>(p, (size_t)32 * n);
+  MergeDesc* mergesAll = carve<MergeDesc>(p, (size_t)32 * (n / 2 + 2));
+  B.info = carve<MergeInfo>(p, (size_t)(n / 2 + 2));
+  GemmDesc<double>* gAll = carve<GemmDesc<double>>(p, (size_t)32 * (n + 4));
+  B.st = st;
+
+  // Host plan: levels bottom-up (deepest first).
+  std::vector<Level> levels;
+  build_levels(0, n, 0, levels);
+  std::reverse(levels.begin(), levels.end());
+  const int L = (int)levels.size();
+  if (L > 32) return cudaErrorInvalidValue;
+
+  // Stage all static per-level data in one pinned buffer, one upload.
+  size_t need = 0;
+  std::vector<size_t> offPos(L), offMer(L), offG(L);
+  std::vector<int> tiles(L);
+  for (int l = 0; l < L; ++l) {
+    offPos[l] = need; need += (size_t)n * sizeof(int);
+    offMer[l] = need; need += levels[l].merges.size() * sizeof(MergeDesc);
+    need = (need + 15) & ~size_t(15);
+    offG[l] = need; need += 2 * levels[l].merges.size() * sizeof(GemmDesc<double>);
+  }
+  if (need > hstage_bytes) return cudaErrorInvalidValue;
+  char* h = reinterpret_cast<char*>(hstage);
+  for (int l = 0; l < L; ++l) {
+    int* pos = reinterpret_cast<int*>(h + offPos[l]);
+    for (int i = 0; i < n; ++i) pos[i] = -1;  // -1: an unmerged leaf at this level
+    const auto& ms = levels[l].merges;
+    std::memcpy(h + offMer[l], ms.data(), ms.size() * sizeof(MergeDesc));
+    GemmDesc<double>* g = reinterpret_cast<GemmDesc<double>*>(h + offG[l]);
+    int tb = 0;
+    for (size_t mi = 0; mi < ms.size(); ++mi) {
+      for (int i = 0; i < ms[mi].n1 + ms[mi].n2; ++i) pos[ms[mi].s + i] = (int)mi;
+      const int nmax = ms[mi].n1 + ms[mi].n2;
+      for (int half = 0; half < 2; ++half) {
+        GemmDesc<double>& gd = g[2 * mi + half];
+        std::memset(&gd, 0, sizeof(gd));
+        gd.lda = n; gd.ldb = n; gd.ldc = n;
+        gd.alpha = 1.0; gd.beta = 0.0;
+        gd.transA = 0; gd.transB = 0; gd.mode = 0;
+        const int mrows = half == 0 ? ms[mi].n1 : ms[mi].n2;
+        gd.tiles_m = (mrows + kGemmBM - 1) / kGemmBM;
+        gd.tiles_n = (nmax + kGemmBN - 1) / kGemmBN;
+        gd.tile_begin = tb;
+        tb += gd.tiles_m * gd.tiles_n;
+      }
+    }
+    tiles[l] = tb;
+  }
+  // Device copies: posMerge / merges / gemm descriptors per level at fixed offsets inside the work area.
+  cudaError_t err;
+  for (int l = 0; l < L; ++l) {
+    const auto& ms = levels[l].merges;
+    err = cudaMemcpyAsync(posAll + (size_t)l * n, h + offPos[l], (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (err != cudaSuccess) return err;
+    err = cudaMemcpyAsync(mergesAll + (size_t)l * (n / 2 + 2), h + offMer[l], ms.size() * sizeof(MergeDesc),
+                          cudaMemcpyHostToDevice, s);
+    if (err != cudaSuccess) return err;
+    err = cudaMemcpyAsync(gAll + (size_t)l * (n + 4), h + offG[l], 2 * ms.size() * sizeof(GemmDesc<double>),
+                          cudaMemcpyHostToDevice, s);
+    if (err != cudaSuccess) return err;
+  }
+
+  dc_scale_kernel<<<1, 1024, 0, s>>>(n, d, e, B.scale);
+  dc_init_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, d, e, B.dd, B.ee, B.scale);
+  {
+    const int blocks = (int)std::min<size_t>((nn + 255) / 256, 4096);
+    dc_identity_kernel<<<blocks, 256, 0, s>>>(n, n, B.Qa, B.Qb, B.dd, dnext);
+  }
+  for (int l = 0; l < L; ++l) {
+    const int nm = (int)levels[l].merges.size();
+    int maxn = 0;
+    for (const auto& m : levels[l].merges) maxn = std::max(maxn, m.n1 + m.n2);
+    B.posMerge = posAll + (size_t)l * n;
+    B.merges = mergesAll + (size_t)l * (n / 2 + 2);
+    B.gdesc = gAll + (size_t)l * (n + 4);
+    const int dthreads = maxn > 512 ? 1024 : (maxn > 128 ? 512 : 128);
+    dc_deflate_kernel<<<nm, dthreads, 0, s>>>(B, nm);
+    dc_rotate_gather_kernel<<<dim3(nm, (maxn + 127) / 128), 128, 0, s>>>(B);
+    const int warps_per_block = 8;
+    const int nblk = (n + warps_per_block - 1) / warps_per_block;
+    dc_secular_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B);
+    dc_zhat_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B);
+    dc_vectors_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B);
+    gemm_grouped_launch<double>(B.gdesc, 2 * nm, tiles[l], s);
+    dc_order_kernel<<<nm, maxn > 256 ? 256 : 128, 0, s>>>(B, dnext);
+    dc_copy_kernel<<<dim3(nm, (maxn + 7) / 8), 128, 0, s>>>(B);
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    // Next level reads (dd, Qa) = (dnext, Qb); the old Qa becomes the next output buffer.
+    std::swap(B.Qa, B.Qb);
+    std::swap(B.dd, dnext);
+  }
+  dc_finish_kernel<<<1024, 256, 0, s>>>(n, B.dd, B.scale, d, B.Qa, n, z, ldz);
+  return cudaGetLastError();
+}
+
+}  // namespace xtbeig

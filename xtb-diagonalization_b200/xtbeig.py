@@ -1,0 +1,259 @@
+"""Python host binding of libxtbeig.so: the C ABI of include/xtb_eig.h through ctypes.
+
+The names and argument meaning follow the reference's exports (Sources/Diagonalization/Exports.swift:6-138: Fortran
+by-reference arguments, column-major arrays, LAPACK semantics) so that callers and tests read like xTB's call sites;
+numpy arrays are passed in Fortran order and the in/out arrays are updated in place, as LAPACK does.  Every call runs
+on the GPU; if the shared library is missing this module raises instead of computing anything on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libxtbeig.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "xtb_eig.h")
+
+_lib = None
+
+_I = C.c_int
+_P = C.c_void_p
+
+
+def header_symbols(path: str = HEADER):
+    """Function names declared in include/xtb_eig.h."""
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(xtb_\w+)\s*\(", text)))
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with xtb-diagonalization_b200/build.py")
+        _lib = C.CDLL(LIB_PATH)
+        _lib.xtb_gpu_last_error.restype = C.c_char_p
+        _lib.xtb_gpu_version.restype = C.c_char_p
+        _lib.xtb_gpu_get_option.restype = C.c_long
+        _lib.xtb_gpu_set_option.argtypes = [C.c_char_p, C.c_long]
+        _lib.xtb_gpu_get_option.argtypes = [C.c_char_p]
+        _lib.xtb_dsyevd_device.argtypes = [_I, _P, _I, _P, _P]
+        _lib.xtb_dsygvd_device.argtypes = [_I, _P, _I, _P, _I, _P, _P]
+        _lib.xtb_dsygvd_density_adjoint.argtypes = [_I, _P, _I, _P, _I, C.c_double, C.c_double, _P, _I, _P, _I, _P,
+                                                    _I, _P, _P, _I]
+        _lib.xtb_dsygvd_batched.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P]
+    return _lib
+
+
+def _ref(v):
+    return C.byref(_I(int(v)))
+
+
+def _p(a):
+    return a.ctypes.data_as(_P)
+
+
+def _f(a, dtype):
+    a = np.asarray(a)
+    if a.dtype != dtype or not a.flags.f_contiguous:
+        raise TypeError(f"expected a Fortran-ordered {np.dtype(dtype).name} array")
+    return a
+
+
+class GPUError(RuntimeError):
+    pass
+
+
+def last_status() -> int:
+    return int(lib().xtb_gpu_last_status())
+
+
+def last_error() -> str:
+    return lib().xtb_gpu_last_error().decode()
+
+
+def _raise_if_failed(name):
+    st = last_status()
+    if st != 0:
+        raise GPUError(f"{name}: {last_error()} (status {st})")
+
+
+def version() -> str:
+    return lib().xtb_gpu_version().decode()
+
+
+def set_option(name: str, value: int) -> None:
+    if lib().xtb_gpu_set_option(name.encode(), int(value)) != 0:
+        raise KeyError(name)
+
+
+def get_option(name: str) -> int:
+    return int(lib().xtb_gpu_get_option(name.encode()))
+
+
+# ---------------------------------------------------------------------------------------------- xtb sytrd.c ABI
+
+def xtb_dsytrd_upper(n, a, lda, d, e, tau, work=None):
+    """call xtb_dsytrd_upper(n, a, lda, d, e, tau, work): in place on a (lda x n), d, e, tau."""
+    _f(a, np.float64)
+    work = np.zeros(max(1, n * 32)) if work is None else work
+    lib().xtb_dsytrd_upper(_ref(n), _p(a), _ref(lda), _p(d), _p(e), _p(tau), _p(work))
+    _raise_if_failed("xtb_dsytrd_upper")
+
+
+def xtb_ssytrd_upper(n, a, lda, d, e, tau, work=None):
+    _f(a, np.float32)
+    work = np.zeros(max(1, n * 32), np.float32) if work is None else work
+    lib().xtb_ssytrd_upper(_ref(n), _p(a), _ref(lda), _p(d), _p(e), _p(tau), _p(work))
+    _raise_if_failed("xtb_ssytrd_upper")
+
+
+def xtb_dsytrd_full(n, a, lda, d, e, tau, work=None):
+    _f(a, np.float64)
+    work = np.zeros(max(1, n * 32)) if work is None else work
+    lib().xtb_dsytrd_full(_ref(n), _p(a), _ref(lda), _p(d), _p(e), _p(tau), _p(work))
+    _raise_if_failed("xtb_dsytrd_full")
+
+
+def xtb_dormtr_upper(n, m, a, lda, tau, z, ldz, work=None):
+    _f(z, np.float64)
+    work = np.zeros(max(1, 32 * (2 * n + 2 * m + 32))) if work is None else work
+    lib().xtb_dormtr_upper(_ref(n), _ref(m), _p(a), _ref(lda), _p(tau), _p(z), _ref(ldz), _p(work))
+    _raise_if_failed("xtb_dormtr_upper")
+
+
+def xtb_sormtr_upper(n, m, a, lda, tau, z, ldz, work=None):
+    _f(z, np.float32)
+    work = np.zeros(max(1, 32 * (2 * n + 2 * m + 32)), np.float32) if work is None else work
+    lib().xtb_sormtr_upper(_ref(n), _ref(m), _p(a), _ref(lda), _p(tau), _p(z), _ref(ldz), _p(work))
+    _raise_if_failed("xtb_sormtr_upper")
+
+
+def xtb_dstedc(n, d, e, z, ldz, work=None, lwork=None, iwork=None, liwork=None) -> int:
+    """call xtb_dstedc(n, d, e, z, ldz, work, lwork, iwork, liwork, info); returns info."""
+    lwork = 1 + 4 * n + n * n if lwork is None else lwork
+    liwork = 3 + 5 * n if liwork is None else liwork
+    work = np.zeros(max(1, lwork)) if work is None else work
+    iwork = np.zeros(max(1, liwork), np.int32) if iwork is None else iwork
+    info = _I(0)
+    lib().xtb_dstedc(_ref(n), _p(d), _p(e), _p(z), _ref(ldz), _p(work), _ref(lwork), _p(iwork), _ref(liwork),
+                     C.byref(info))
+    return info.value
+
+
+def xtb_sstedc(n, d, e, z, ldz, work=None, lwork=None, iwork=None, liwork=None) -> int:
+    lwork = 1 + 4 * n + n * n if lwork is None else lwork
+    liwork = 3 + 5 * n if liwork is None else liwork
+    work = np.zeros(max(1, lwork), np.float32) if work is None else work
+    iwork = np.zeros(max(1, liwork), np.int32) if iwork is None else iwork
+    info = _I(0)
+    lib().xtb_sstedc(_ref(n), _p(d), _p(e), _p(z), _ref(ldz), _p(work), _ref(lwork), _p(iwork), _ref(liwork),
+                     C.byref(info))
+    return info.value
+
+
+def xtb_dsymmetrize_pad(n, src, lds, dst, ldd):
+    lib().xtb_dsymmetrize_pad(_ref(n), _p(src), _ref(lds), _p(dst), _ref(ldd))
+    _raise_if_failed("xtb_dsymmetrize_pad")
+
+
+# ---------------------------------------------------------------------------------------------- whole solves
+
+def dsyevd(a, jobz="V", uplo="U"):
+    """LAPACK dsyevd on the GPU: returns (w, z or None, info); a is not modified."""
+    a = np.array(a, dtype=np.float64, order="F", copy=True)
+    n = a.shape[0]
+    w = np.zeros(n)
+    info = _I(0)
+    lib().xtb_dsyevd_gpu(jobz.encode(), uplo.encode(), _ref(n), _p(a), _ref(max(1, n)), _p(w), None, _ref(1), None,
+                         _ref(1), C.byref(info))
+    return w, (a if jobz.upper() == "V" else None), info.value
+
+
+def dsygvd(a, b, jobz="V", uplo="U"):
+    """LAPACK dsygvd (itype 1) on the GPU: returns (w, C, factor, info); inputs are not modified."""
+    a = np.array(a, dtype=np.float64, order="F", copy=True)
+    b = np.array(b, dtype=np.float64, order="F", copy=True)
+    n = a.shape[0]
+    w = np.zeros(n)
+    info = _I(0)
+    lib().xtb_dsygvd_gpu(_ref(1), jobz.encode(), uplo.encode(), _ref(n), _p(a), _ref(max(1, n)), _p(b),
+                         _ref(max(1, n)), _p(w), None, _ref(1), None, _ref(1), C.byref(info))
+    return w, a, b, info.value
+
+
+def dsygvd_device(n, a_ptr, lda, b_ptr, ldb, w_ptr, stream=0) -> int:
+    """Device-pointer solve (column-major device buffers, e.g. torch tensors' data_ptr())."""
+    return int(lib().xtb_dsygvd_device(int(n), _P(a_ptr), int(lda), _P(b_ptr), int(ldb), _P(w_ptr),
+                                       _P(stream) if stream else None))
+
+
+def dsyevd_device(n, a_ptr, lda, w_ptr, stream=0) -> int:
+    return int(lib().xtb_dsyevd_device(int(n), _P(a_ptr), int(lda), _P(w_ptr), _P(stream) if stream else None))
+
+
+def dsygvd_batched(hs, ss):
+    """Batch of generalized problems; returns lists (w_i, C_i, U_i) and the info array."""
+    count = len(hs)
+    a = [np.array(h, dtype=np.float64, order="F", copy=True) for h in hs]
+    b = [np.array(s, dtype=np.float64, order="F", copy=True) for s in ss]
+    ns = np.array([x.shape[0] for x in a], np.int32)
+    w = [np.zeros(x.shape[0]) for x in a]
+    ap = (C.c_void_p * count)(*[x.ctypes.data for x in a])
+    bp = (C.c_void_p * count)(*[x.ctypes.data for x in b])
+    wp = (C.c_void_p * count)(*[x.ctypes.data for x in w])
+    info = np.zeros(count, np.int32)
+    lib().xtb_dsygvd_batched(count, _p(ns), ap, _p(ns), bp, _p(ns), wp, _p(info))
+    return w, a, b, info
+
+
+def density_adjoint(h, s, kt, mu, wbar):
+    """dL/dH, dL/dS of L = sum(wbar o P), P = C diag(2/(1+exp((e-mu)/kT))) C^T; returns (dH, dS, e, C, info)."""
+    h = np.asfortranarray(h, dtype=np.float64)
+    s = np.asfortranarray(s, dtype=np.float64)
+    wbar = np.asfortranarray(wbar, dtype=np.float64)
+    n = h.shape[0]
+    dh = np.zeros((n, n), order="F")
+    ds = np.zeros((n, n), order="F")
+    e = np.zeros(n)
+    c = np.zeros((n, n), order="F")
+    info = lib().xtb_dsygvd_density_adjoint(n, _p(h), n, _p(s), n, float(kt), float(mu), _p(wbar), n, _p(dh), n,
+                                            _p(ds), n, _p(e), _p(c), n)
+    return dh, ds, e, c, int(info)
+
+
+# ---------------------------------------------------------------------------------------------- convenience
+
+def sytrd_upper(a, dtype=np.float64):
+    """Functional form: returns (A_out, d, e, tau) like oracle.lapack.sytrd_upper."""
+    a = np.array(a, dtype=dtype, order="F", copy=True)
+    n = a.shape[0]
+    d = np.zeros(max(n, 1), dtype)
+    e = np.zeros(max(n - 1, 1), dtype)
+    tau = np.zeros(max(n - 1, 1), dtype)
+    (xtb_dsytrd_upper if dtype == np.float64 else xtb_ssytrd_upper)(n, a, n, d, e, tau)
+    return a, d[:n], e[: max(n - 1, 0)], tau[: max(n - 1, 0)]
+
+
+def stedc(d, e, dtype=np.float64):
+    d = np.array(d, dtype=dtype, copy=True)
+    n = d.shape[0]
+    ee = np.zeros(max(n - 1, 1), dtype)
+    ee[: n - 1] = np.asarray(e, dtype)[: n - 1]
+    z = np.zeros((n, n), dtype, order="F")
+    info = (xtb_dstedc if dtype == np.float64 else xtb_sstedc)(n, d, ee, z, max(n, 1))
+    return d, z, info
+
+
+def ormtr_upper(a, tau, z, dtype=np.float64):
+    a = np.array(a, dtype=dtype, order="F", copy=True)
+    z = np.array(z, dtype=dtype, order="F", copy=True)
+    n, m = z.shape
+    tt = np.zeros(max(n - 1, 1), dtype)
+    tt[: n - 1] = np.asarray(tau, dtype)[: n - 1]
+    (xtb_dormtr_upper if dtype == np.float64 else xtb_sormtr_upper)(n, m, a, n, tt, z, n)
+    return z
