@@ -199,6 +199,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_grouped_kernel(const GemmDe
       for (int c = 0; c < 2; ++c) {
         const int gn = n0 + wn * 32 + j * 8 + c2 + c;
         if (gn >= p.N) continue;
+        if ((p.mode & kCUpper) && gm > gn) continue;  // kCUpper updates the upper triangle only
         T* dst = p.C + gm + (size_t)gn * p.ldc;
         T v = alpha * acc[i][j][c];
         if (beta != T(0)) v += beta * *dst;
