@@ -1,0 +1,346 @@
+"""Benchmark: milliseconds per n = 1788 generalized eigensolve (sygvd, H C = S C e, all eigenpairs) on a B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 1788]
+
+Workload: the generalized construction with n = 1788, seed 2 (S = I + banded random overlap with lambda_min >= 0.05,
+H = S^1/2 Q diag(lam) Q^T S^1/2, lam ~ U[-1.0, 0.5] Eh with a 0.05 Eh HOMO/LUMO gap at n/2), FP64 throughout on the
+GPU (potrf -> X = U^-1 -> X^T H X -> resident sytrd -> divide-and-conquer stedc -> compact-WY ormtr -> X C').
+Synthetic seeded inputs stand in for the GFN2 H/S dumps the reference reads (none are published).
+
+ours (default):  one step = restore H, S on the device (D2D copy of pristine inputs) + one device-pointer solve on
+    torch's current stream, timed with CUDA events per step; L2 is flushed (256 MB write) before every timed step,
+    outside the events.  `value` = mean ms per solve (whole job: summed over replicas for N > 1, see DESIGN.md:
+    single solves do not shard, ranks are independent replicas).  `e2e` = the same solve through the C ABI with
+    pinned HOST buffers (H2D of H and S, D2H of C, U and e inside the timed region).  `roofline` = the resident
+    reduction kernel (sytrd): algorithmic bytes 4 n^3 / 3 (its symv reads n^3/6 FP64 elements) / its event-timed
+    duration, against the measured HBM copy bandwidth.  `cpu_baseline` = the reference's LAPACK chain (dpotrf, dsygst,
+    dsytrd, dstedc, dormtr, dtrsm from OpenBLAS) on the host cores, rank 0, bounded sample.
+reference:  the same LAPACK chain on the host cores only (rank 0; other ranks exit), the reference's CPU path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "xtb-diagonalization_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "ms per n=1788 generalized eigensolve (sygvd, all eigenpairs)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1788)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-budget-s", type=float, default=20.0, help="bound on the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+# ------------------------------------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+# ------------------------------------------------------------------------------------------------ CPU path
+
+def cpu_chain_time(h, s, budget_s: float, max_runs: int):
+    """The reference's LAPACK chain on the host: ms per solve over a bounded sample, and the thread count used."""
+    import numpy as np
+
+    from oracle import lapack
+
+    threads = lapack.get_threads()
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < max_runs and (not times or time.perf_counter() < t_end):
+        t0 = time.perf_counter()
+        w, c = lapack.sygvd_chain(h, s)
+        times.append((time.perf_counter() - t0) * 1e3)
+    assert np.all(np.isfinite(w))
+    return statistics.median(times), len(times), threads
+
+
+def run_reference(args):
+    rank, _, world = rank_info()
+    if rank != 0:
+        return
+    from oracle import inputs
+
+    h, s, _ = inputs.generalized(args.n, seed=args.seed)
+    from oracle import lapack
+
+    for _ in range(max(0, min(args.warmup, 1))):
+        lapack.sygvd_chain(h, s)
+    budget = 150.0
+    ms, runs, threads = cpu_chain_time(h, s, budget, max(1, args.steps))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world,
+        "steps": runs, "warmup": min(args.warmup, 1), "ms_per_step": round(ms, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generalized H, S)",
+        "config": {"workload": f"generalized eigensolve n={args.n} seed={args.seed}, all eigenpairs, FP64",
+                   "path": "LAPACK dpotrf,dsygst,dsytrd,dstedc,dormtr,dtrsm (OpenBLAS 0.3.30 from scipy)",
+                   "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": threads, "kind": "port",
+                         "sample": f"median of {runs} full solves (bounded to ~{int(budget)} s)"},
+        "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------ GPU path
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            pk = json.load(f)
+        return float(pk.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(n):
+    """DRAM bytes per sytrd launch from the committed ncu summary (profiles/traffic.json), scaled to n if captured on
+    a smaller case; None if no capture exists."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        t = json.load(f)
+    rec = t.get("sytrd")
+    if not rec:
+        return None
+    return float(rec["bytes_per_launch"]) * (n / rec["n"]) ** 3 if rec.get("n") else None
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import xtbeig
+    from oracle import inputs
+
+    rank, local_rank, world = rank_info()
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local_rank)
+    xtbeig.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n = args.n
+    h_np, s_np, lam = inputs.generalized(n, seed=args.seed + rank * 0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    H0 = torch.from_numpy(np.ascontiguousarray(h_np)).to(dev)  # symmetric: row-major == column-major
+    S0 = torch.from_numpy(np.ascontiguousarray(s_np)).to(dev)
+    H = torch.empty_like(H0)
+    S = torch.empty_like(S0)
+    W = torch.empty(n, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def solve():
+        H.copy_(H0)
+        S.copy_(S0)
+        info = xtbeig.dsygvd_device(n, H.data_ptr(), n, S.data_ptr(), n, W.data_ptr(), stream.cuda_stream)
+        if info != 0:
+            raise RuntimeError(f"xtb_dsygvd_device info={info}: {xtbeig.last_error()}")
+
+    for _ in range(max(3, args.warmup)):
+        solve()
+    torch.cuda.synchronize(dev)
+    # accuracy of the measured configuration (outside the timed region)
+    w = W.cpu().numpy()
+    eig_err = float(np.max(np.abs(w - lam)))
+
+    # Stage times of one untimed solve (CUDA events at stage boundaries inside the library).
+    xtbeig.set_option("stage_timing", 1)
+    flush.zero_()
+    solve()
+    stages = xtbeig.stage_times()
+    xtbeig.set_option("stage_timing", 0)
+
+    # Timed region.
+    gpu_uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    sampler = ClockSampler(("GPU-" + gpu_uuid) if not gpu_uuid.startswith("GPU-") else gpu_uuid)
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = xtbeig.launch_count()
+    sampler.start()
+    time.sleep(0.3)
+    t_wall0 = time.perf_counter()
+    for i in range(K):
+        flush.zero_()
+        ev[i][0].record(stream)
+        solve()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize(dev)
+    t_wall = time.perf_counter() - t_wall0
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    launches = xtbeig.launch_count() - launches0
+    per = [a.elapsed_time(b) for a, b in ev]
+    ms_step = sum(per) / K
+    t = torch.tensor([ms_step], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_step_max = float(t.item())
+
+    # End to end through the C ABI with pinned host buffers.
+    import ctypes
+
+    L = xtbeig.lib()
+    hp = torch.empty((n, n), dtype=torch.float64, pin_memory=True).numpy()
+    sp = torch.empty((n, n), dtype=torch.float64, pin_memory=True).numpy()
+    wp = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    hf, sf = np.ascontiguousarray(h_np), np.ascontiguousarray(s_np)
+    info = ctypes.c_int(0)
+    one = ctypes.c_int(1)
+    e2e = []
+    for i in range(args.e2e_steps + 2):
+        np.copyto(hp, hf)
+        np.copyto(sp, sf)
+        t0 = time.perf_counter()
+        L.xtb_dsygvd_gpu(ctypes.byref(one), b"V", b"U", ctypes.byref(ctypes.c_int(n)), xtbeig._p(hp),
+                         ctypes.byref(ctypes.c_int(n)), xtbeig._p(sp), ctypes.byref(ctypes.c_int(n)), xtbeig._p(wp),
+                         None, ctypes.byref(one), None, ctypes.byref(one), ctypes.byref(info))
+        dt = (time.perf_counter() - t0) * 1e3
+        if info.value != 0:
+            raise RuntimeError(f"xtb_dsygvd_gpu info={info.value}: {xtbeig.last_error()}")
+        if i >= 2:
+            e2e.append(dt)
+    e2e_ms = statistics.median(e2e)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_ms = float(te.item())
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        t_sytrd = dict(stages).get("sytrd")
+        alg_bytes = 4.0 * n ** 3 / 3.0
+        achieved = alg_bytes / (t_sytrd * 1e-3) / 1e9 if t_sytrd else None
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            ms_cpu, runs, threads = cpu_chain_time(h_np, s_np, args.cpu_budget_s, 50)
+            cpu = {"value": round(ms_cpu, 3), "unit": "ms", "cores": threads, "kind": "port",
+                   "sample": f"median of {runs} full n={n} solves of the LAPACK chain (OpenBLAS), <= "
+                             f"{args.cpu_budget_s:.0f} s"}
+        total_stage = sum(v for _, v in stages) or 1.0
+        line = {
+            "metric": METRIC, "value": round(ms_step_max / world, 4), "unit": "ms", "n_gpus": world, "steps": K,
+            "warmup": max(3, args.warmup), "ms_per_step": round(ms_step_max, 4), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generalized H, S; exact spectrum known)",
+            "config": {"workload": f"generalized eigensolve n={n} seed={args.seed}, all eigenpairs, FP64 path",
+                       "path": "potrf, trtri, X^T H X, resident sytrd, D&C stedc, WY ormtr, X C' (all CUDA)",
+                       "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}",
+                       "eigenvalue_error_vs_exact": eig_err, "wall_s_timed_region": round(t_wall, 3)},
+            "roofline": {"bound": "hbm", "kernel": "sytrd_resident_kernel",
+                         "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4) if achieved else None, "traffic": load_traffic(n),
+                         "peak_kind": f"{peak_kind} copy bandwidth",
+                         "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": t_sytrd},
+            "stages_ms": {k: round(v, 4) for k, v in stages},
+            "stage_share": {k: round(v / total_stage, 3) for k, v in stages},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_ms / world, 4), "unit": "ms",
+                    "h2d_bytes_per_step": 2 * n * n * 8, "d2h_bytes_per_step": (2 * n * n + n) * 8 + 16,
+                    "per_replica_ms": round(e2e_ms, 4)},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

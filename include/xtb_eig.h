@@ -68,7 +68,7 @@ void xtb_dsygvd_gpu(const int* itype, const char* jobz, const char* uplo, const 
                     const int* liwork, int* info);
 
 /* Device-pointer variants (by value; uplo 'U'; vectors always computed).  All pointers are device memory of the
- * current device; `stream` is a cudaStream_t (NULL: the calling thread's library stream).  The call returns after
+ * current device; `stream` is a cudaStream_t on which the work is queued (NULL: the legacy default stream).  The call returns after
  * queueing the work, except that it synchronises the stream once at the end to read the device status; it returns
  * LAPACK-style info. */
 int xtb_dsyevd_device(int n, double* a, int lda, double* w, void* stream);
@@ -89,10 +89,21 @@ int xtb_dsygvd_density_adjoint(int n, const double* h, int ldh, const double* s,
                                double* c_out, int ldc);
 
 /* Options (process-wide): "sytrd_grid" (CTAs of the resident reduction, 0 = auto), "ormtr_nb" (reflectors per
- * compact-WY block, default 128), "wait_limit_ms" (device wait time limit, default 2000).  Returns 0, or -1 for an
- * unknown name. */
+ * compact-WY block, default 128), "wait_limit_ms" (device wait time limit, default 2000), "stage_timing" (1: record
+ * CUDA events at stage boundaries; read with xtb_gpu_stage_*).  Returns 0, or -1 for an unknown name. */
 int xtb_gpu_set_option(const char* name, long value);
 long xtb_gpu_get_option(const char* name);
+
+/* Device of the calling thread's later calls (the library keeps its own CUDA runtime state, so a caller that selects
+ * devices through another runtime, e.g. a Python framework, states the device here).  Returns 0 or -1000 - code. */
+int xtb_gpu_set_device(int device);
+
+/* Stage times of the calling thread's last call (with the "stage_timing" option on): count, names, milliseconds. */
+int xtb_gpu_stage_count(void);
+const char* xtb_gpu_stage_name(int i);
+double xtb_gpu_stage_ms(int i);
+/* Kernel launches issued by the library so far (all threads). */
+long long xtb_gpu_launch_count(void);
 
 /* Last status of the calling thread: 0 or a failure code; message for humans. */
 int xtb_gpu_last_status(void);

@@ -75,19 +75,19 @@ cudaError_t dk_adjoint(int n, const double* c, const double* e, double mu, doubl
   const size_t total = (size_t)n * n;
   const int grid = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
   // G1 -> t1, G2 -> t3
-  dk_weights_kernel<<<grid, 256, 0, s>>>(n, e, mu, kt, t2, t1, t3);
+  dk_weights_kernel<<<grid, 256, 0, s>>>(n, e, mu, kt, t2, t1, t3); note_launches();
   // dH = C G1 C^T
   p = gemm_problem<double>(n, n, n, 1.0, c, n, 0, t1, n, 0, 0.0, t2, n);
   if ((err = gemm_group<double>(arena, &p, 1, s)) != cudaSuccess) return err;
   p = gemm_problem<double>(n, n, n, 1.0, t2, n, 0, c, n, 1, 0.0, t1, n);
   if ((err = gemm_group<double>(arena, &p, 1, s)) != cudaSuccess) return err;
-  sym_average_kernel<<<grid, 256, 0, s>>>(n, t1, 1.0, dh, n);
+  sym_average_kernel<<<grid, 256, 0, s>>>(n, t1, 1.0, dh, n); note_launches();
   // dS = -C G2 C^T
   p = gemm_problem<double>(n, n, n, 1.0, c, n, 0, t3, n, 0, 0.0, t2, n);
   if ((err = gemm_group<double>(arena, &p, 1, s)) != cudaSuccess) return err;
   p = gemm_problem<double>(n, n, n, 1.0, t2, n, 0, c, n, 1, 0.0, t1, n);
   if ((err = gemm_group<double>(arena, &p, 1, s)) != cudaSuccess) return err;
-  sym_average_kernel<<<grid, 256, 0, s>>>(n, t1, -1.0, ds, n);
+  sym_average_kernel<<<grid, 256, 0, s>>>(n, t1, -1.0, ds, n); note_launches();
   return cudaGetLastError();
 }
 

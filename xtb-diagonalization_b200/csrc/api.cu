@@ -25,6 +25,8 @@ namespace {
 std::atomic<long> g_sytrd_grid{0};
 std::atomic<long> g_ormtr_nb{128};
 std::atomic<long> g_wait_ms{2000};
+std::atomic<long> g_stage_timing{0};
+std::atomic<long long> g_launches{0};
 
 struct Buf {
   void* p = nullptr;
@@ -40,12 +42,14 @@ struct Context {
   DescArena arena;
   DeviceStatus* d_status = nullptr;
   DeviceStatus* h_status = nullptr;
+  std::vector<cudaEvent_t> events;  // pool for stage timing
 };
 
 struct ThreadState {
   std::map<int, Context*> ctx;  // by device; contexts live until process exit
   int last_code = 0;
   std::string last_msg;
+  std::vector<std::pair<std::string, double>> stages;  // last call's stage times (ms), when stage timing is on
 };
 
 thread_local ThreadState t_state;
@@ -96,9 +100,29 @@ struct Call {
   const char* where = "";
   bool ok() const { return err == cudaSuccess; }
 
-  Call(Context* ctx, cudaStream_t user) : c(ctx), s(user ? user : ctx->stream) {
+  std::vector<std::pair<const char*, cudaEvent_t>> marks;
+  bool timing = false;
+
+  // Host-pointer calls run on the context's own stream; device-pointer calls on the caller's stream, where NULL is the
+  // CUDA legacy default stream (ordered with the caller's other work on blocking streams).
+  Call(Context* ctx, cudaStream_t user, bool caller_stream = false)
+      : c(ctx), s(caller_stream ? user : ctx->stream) {
     c->arena.reset();
+    timing = g_stage_timing.load() != 0;
     check(cudaMemsetAsync(c->d_status, 0, sizeof(DeviceStatus), s), "status reset");
+    mark("begin");
+  }
+  // Stage boundary: with stage timing on, an event on the call's stream; finish() turns consecutive events into
+  // per-stage milliseconds (the GPU counterpart of the reference's per-stage timing callback).
+  void mark(const char* name) {
+    if (!timing || !ok()) return;
+    const size_t i = marks.size();
+    while (c->events.size() <= i) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return;
+      c->events.push_back(e);
+    }
+    if (cudaEventRecord(c->events[i], s) == cudaSuccess) marks.emplace_back(name, c->events[i]);
   }
   bool check(cudaError_t e, const char* w) {
     if (err == cudaSuccess && e != cudaSuccess) {
@@ -159,6 +183,12 @@ struct Call {
     if (!ok()) {
       record(-1000 - (int)err, std::string("CUDA error at ") + where + ": " + cudaGetErrorString(err));
       return -1000 - (int)err;
+    }
+    t_state.stages.clear();
+    for (size_t i = 1; i < marks.size(); ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, marks[i - 1].second, marks[i].second);
+      t_state.stages.emplace_back(marks[i].first, (double)ms);
     }
     DeviceStatus st = *c->h_status;
     if (out) *out = st;
@@ -250,19 +280,26 @@ void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
   double* tau = k.template dev<double>("gv.tau", (size_t)n);
   if (!k.ok()) return;
   k.check(potrf_upper(n, u, n, k.c->d_status, k.c->arena, k.s), "potrf");
+  k.mark("potrf");
   if (k.ok()) k.check(trtri_upper(n, u, n, x, n, t, k.c->arena, k.s), "trtri");
+  k.mark("trtri");
   // G = H X (X upper), then H' = X^T G on the upper tiles, symmetrised for the reduction.
   GemmDesc<double> p = gemm_problem<double>(n, n, n, 1.0, h, n, 0, x, n, 0, 0.0, t, n, kTriBUpper);
   if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "congruence 1");
   p = gemm_problem<double>(n, n, n, 1.0, x, n, 1, t, n, 0, 0.0, hp, n, kTriALower | kCUpper);
   if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "congruence 2");
   if (k.ok()) symmetrize_upper<double>(n, hp, n, h, n, k.s);
+  k.mark("congruence");
   stage_sytrd<double>(k, n, h, n, r, n, w, e, tau);
+  k.mark("sytrd");
   stage_stedc(k, n, w, e, z, n);
+  k.mark("stedc");
   stage_ormtr<double>(k, n, n, r, n, tau, z, n);
+  k.mark("ormtr");
   // C = X Z (X upper).
   p = gemm_problem<double>(n, n, n, 1.0, x, n, 0, z, n, 0, 0.0, c, n, kTriAUpper);
   if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "back-transform");
+  k.mark("trmm");
 }
 
 // Standard problem on device buffers: f (n x n full symmetric, ld n) consumed; z (n x n) eigenvectors; w eigenvalues.
@@ -273,8 +310,11 @@ void core_syevd(Call& k, int n, double* f, double* z, double* w, bool vectors) {
   double* tau = k.template dev<double>("ev.tau", (size_t)n);
   if (!k.ok()) return;
   stage_sytrd<double>(k, n, f, n, r, n, w, e, tau);
+  k.mark("sytrd");
   stage_stedc(k, n, w, e, z, n);
+  k.mark("stedc");
   if (vectors) stage_ormtr<double>(k, n, n, r, n, tau, z, n);
+  k.mark("ormtr");
 }
 
 int info_of(int code, const DeviceStatus& st, int n) {
@@ -395,6 +435,9 @@ void stedc_host(const int* n_, T* d, T* e, T* z, const int* ldz_, T* work, const
 }
 
 }  // namespace
+
+void note_launches(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
 }  // namespace xtbeig
 
 using namespace xtbeig;
@@ -557,7 +600,7 @@ int xtb_dsyevd_device(int n, double* a, int lda, double* w, void* stream) {
   if (n == 0) return 0;
   Context* c = context();
   if (!c) return t_state.last_code;
-  Call k(c, (cudaStream_t)stream);
+  Call k(c, (cudaStream_t)stream, true);
   double* df = k.dev<double>("dv.F", (size_t)n * n);
   double* dz = k.dev<double>("dv.Z", (size_t)n * n);
   if (k.ok()) symmetrize_upper<double>(n, a, lda, df, n, k.s);
@@ -575,7 +618,7 @@ int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, 
   if (n == 0) return 0;
   Context* c = context();
   if (!c) return t_state.last_code;
-  Call k(c, (cudaStream_t)stream);
+  Call k(c, (cudaStream_t)stream, true);
   double* dh = k.dev<double>("dv.F", (size_t)n * n);
   double* du = k.dev<double>("dv.U", (size_t)n * n);
   double* dc = k.dev<double>("dv.C", (size_t)n * n);
@@ -673,6 +716,7 @@ int xtb_gpu_set_option(const char* name, long value) {
   if (!std::strcmp(name, "sytrd_grid")) { g_sytrd_grid = value; return 0; }
   if (!std::strcmp(name, "ormtr_nb")) { g_ormtr_nb = value; return 0; }
   if (!std::strcmp(name, "wait_limit_ms")) { g_wait_ms = value; return 0; }
+  if (!std::strcmp(name, "stage_timing")) { g_stage_timing = value; return 0; }
   return -1;
 }
 
@@ -681,8 +725,30 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "sytrd_grid")) return g_sytrd_grid;
   if (!std::strcmp(name, "ormtr_nb")) return g_ormtr_nb;
   if (!std::strcmp(name, "wait_limit_ms")) return g_wait_ms;
+  if (!std::strcmp(name, "stage_timing")) return g_stage_timing;
   return -1;
 }
+
+int xtb_gpu_set_device(int device) {
+  const cudaError_t err = cudaSetDevice(device);
+  if (err != cudaSuccess) {
+    record(-1000 - (int)err, std::string("cudaSetDevice failed: ") + cudaGetErrorString(err));
+    return -1000 - (int)err;
+  }
+  return 0;
+}
+
+int xtb_gpu_stage_count(void) { return (int)t_state.stages.size(); }
+
+const char* xtb_gpu_stage_name(int i) {
+  return (i >= 0 && i < (int)t_state.stages.size()) ? t_state.stages[i].first.c_str() : "";
+}
+
+double xtb_gpu_stage_ms(int i) {
+  return (i >= 0 && i < (int)t_state.stages.size()) ? t_state.stages[i].second : -1.0;
+}
+
+long long xtb_gpu_launch_count(void) { return g_launches.load(); }
 
 int xtb_gpu_last_status(void) { return t_state.last_code; }
 

@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_grouped_kernel(const GemmDe
 template <typename T>
 void gemm_grouped_launch(const GemmDesc<T>* d_descs, int nprob, int total_tiles, cudaStream_t s) {
   if (nprob <= 0 || total_tiles <= 0) return;
-  gemm_grouped_kernel<T><<<total_tiles, kGemmThreads, 0, s>>>(d_descs, nprob);
+  gemm_grouped_kernel<T><<<total_tiles, kGemmThreads, 0, s>>>(d_descs, nprob); note_launches();
 }
 
 template void gemm_grouped_launch<double>(const GemmDesc<double>*, int, int, cudaStream_t);

@@ -9,6 +9,9 @@
 
 namespace xtbeig {
 
+// Count of kernel launches issued by the library (all threads); read through xtb_gpu_launch_count().
+void note_launches(int k = 1);
+
 // ---------------------------------------------------------------------------------------------------- sytrd
 template <typename T>
 struct SytrdParams {

@@ -100,7 +100,7 @@ cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, i
   {
     const size_t total = (size_t)n * nm1;
     int grid = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
-    build_v_kernel<T><<<grid, 256, 0, s>>>(n, a, lda, w.V);
+    build_v_kernel<T><<<grid, 256, 0, s>>>(n, a, lda, w.V); note_launches();
   }
   // Gram matrices of all blocks, one grouped launch.
   GemmDesc<T>* probs = new GemmDesc<T>[nblocks];
@@ -115,7 +115,7 @@ cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, i
     const size_t smem = ((size_t)nb * nb + nb) * sizeof(T);
     err = cudaFuncSetAttribute(wy_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) { delete[] probs; return err; }
-    wy_factor_kernel<T><<<nblocks, 128, smem, s>>>(nm1, nb, tau, w.Tf);
+    wy_factor_kernel<T><<<nblocks, 128, smem, s>>>(nm1, nb, tau, w.Tf); note_launches();
   }
   // Y_b = V_b T_b^T (op(B) = T_b^T is lower triangular).
   for (int b = 0; b < nblocks; ++b) {

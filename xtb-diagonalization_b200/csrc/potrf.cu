@@ -125,10 +125,10 @@ cudaError_t potrf_upper(int n, double* a, int lda, DeviceStatus* st, DescArena& 
   if (err != cudaSuccess) return err;
   for (int j = 0; j < n; j += NB) {
     const int nb = std::min(NB, n - j);
-    potrf_diag_kernel<<<1, 256, 0, s>>>(n, a, lda, j, st);
+    potrf_diag_kernel<<<1, 256, 0, s>>>(n, a, lda, j, st); note_launches();
     const int rest = n - j - nb;
     if (rest <= 0) break;
-    potrf_trsm_kernel<<<(rest + trsm_threads - 1) / trsm_threads, trsm_threads, trsm_smem, s>>>(n, a, lda, j, st);
+    potrf_trsm_kernel<<<(rest + trsm_threads - 1) / trsm_threads, trsm_threads, trsm_smem, s>>>(n, a, lda, j, st); note_launches();
     // A22 -= U12^T U12 (upper tiles only).
     double* u12 = a + j + (size_t)(j + nb) * lda;
     double* a22 = a + (j + nb) + (size_t)(j + nb) * lda;
@@ -145,7 +145,7 @@ cudaError_t trtri_upper(int n, const double* u, int ldu, double* x, int ldx, dou
   cudaError_t err = cudaMemsetAsync(x, 0, sizeof(double) * ((size_t)ldx * (n - 1) + n), s);
   if (err != cudaSuccess) return err;
   const int nblk = (n + NB - 1) / NB;
-  trtri_diag_kernel<<<nblk, 128, 0, s>>>(n, u, ldu, x, ldx);
+  trtri_diag_kernel<<<nblk, 128, 0, s>>>(n, u, ldu, x, ldx); note_launches();
   std::vector<GemmDesc<double>> p1, p2;
   for (int sz = NB; sz < n; sz *= 2) {
     p1.clear();

@@ -714,11 +714,11 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
     if (err != cudaSuccess) return err;
   }
 
-  dc_scale_kernel<<<1, 1024, 0, s>>>(n, d, e, B.scale);
-  dc_init_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, d, e, B.dd, B.ee, B.scale);
+  dc_scale_kernel<<<1, 1024, 0, s>>>(n, d, e, B.scale); note_launches();
+  dc_init_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, d, e, B.dd, B.ee, B.scale); note_launches();
   {
     const int blocks = (int)std::min<size_t>((nn + 255) / 256, 4096);
-    dc_identity_kernel<<<blocks, 256, 0, s>>>(n, n, B.Qa, B.Qb, B.dd, dnext);
+    dc_identity_kernel<<<blocks, 256, 0, s>>>(n, n, B.Qa, B.Qb, B.dd, dnext); note_launches();
   }
   for (int l = 0; l < L; ++l) {
     const int nm = (int)levels[l].merges.size();
@@ -728,23 +728,23 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
     B.merges = mergesAll + (size_t)l * (n / 2 + 2);
     B.gdesc = gAll + (size_t)l * (n + 4);
     const int dthreads = maxn > 512 ? 1024 : (maxn > 128 ? 512 : 128);
-    dc_deflate_kernel<<<nm, dthreads, 0, s>>>(B, nm);
-    dc_rotate_gather_kernel<<<dim3(nm, (maxn + 127) / 128), 128, 0, s>>>(B);
+    dc_deflate_kernel<<<nm, dthreads, 0, s>>>(B, nm); note_launches();
+    dc_rotate_gather_kernel<<<dim3(nm, (maxn + 127) / 128), 128, 0, s>>>(B); note_launches();
     const int warps_per_block = 8;
     const int nblk = (n + warps_per_block - 1) / warps_per_block;
-    dc_secular_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B);
-    dc_zhat_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B);
-    dc_vectors_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B);
+    dc_secular_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();
+    dc_zhat_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();
+    dc_vectors_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();
     gemm_grouped_launch<double>(B.gdesc, 2 * nm, tiles[l], s);
-    dc_order_kernel<<<nm, maxn > 256 ? 256 : 128, 0, s>>>(B, dnext);
-    dc_copy_kernel<<<dim3(nm, (maxn + 7) / 8), 128, 0, s>>>(B);
+    dc_order_kernel<<<nm, maxn > 256 ? 256 : 128, 0, s>>>(B, dnext); note_launches();
+    dc_copy_kernel<<<dim3(nm, (maxn + 7) / 8), 128, 0, s>>>(B); note_launches();
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     // Next level reads (dd, Qa) = (dnext, Qb); the old Qa becomes the next output buffer.
     std::swap(B.Qa, B.Qb);
     std::swap(B.dd, dnext);
   }
-  dc_finish_kernel<<<1024, 256, 0, s>>>(n, B.dd, B.scale, d, B.Qa, n, z, ldz);
+  dc_finish_kernel<<<1024, 256, 0, s>>>(n, B.dd, B.scale, d, B.Qa, n, z, ldz); note_launches();
   return cudaGetLastError();
 }
 

@@ -129,59 +129,71 @@ template <typename T>
 void symmetrize_upper(int n, const T* src, int lds, T* dst, int ldd, cudaStream_t s) {
   if (n <= 0) return;
   const int t = (n + TILE - 1) / TILE;
-  symmetrize_kernel<T, false><<<dim3(t, t), dim3(TILE, 8), 0, s>>>(n, src, lds, dst, ldd);
+  symmetrize_kernel<T, false><<<dim3(t, t), dim3(TILE, 8), 0, s>>>(n, src, lds, dst, ldd); note_launches();
 }
 
 template <typename T>
 void symmetrize_lower(int n, const T* src, int lds, T* dst, int ldd, cudaStream_t s) {
   if (n <= 0) return;
   const int t = (n + TILE - 1) / TILE;
-  symmetrize_kernel<T, true><<<dim3(t, t), dim3(TILE, 8), 0, s>>>(n, src, lds, dst, ldd);
+  symmetrize_kernel<T, true><<<dim3(t, t), dim3(TILE, 8), 0, s>>>(n, src, lds, dst, ldd); note_launches();
 }
 
 template <typename T>
 void upper_transpose_to_lower(int n, const T* src, int lds, T* dst, int ldd, cudaStream_t s) {
   if (n <= 0) return;
   const int t = (n + TILE - 1) / TILE;
-  upper_transpose_kernel<T><<<dim3(t, t), dim3(TILE, 8), 0, s>>>(n, src, lds, dst, ldd);
+  upper_transpose_kernel<T><<<dim3(t, t), dim3(TILE, 8), 0, s>>>(n, src, lds, dst, ldd); note_launches();
 }
 
 template <typename T>
 void mirror_upper_inplace(int n, T* a, int lda, cudaStream_t s) {
   if (n <= 0) return;
   const int t = (n + TILE - 1) / TILE;
-  mirror_kernel<T><<<dim3(t, t), dim3(TILE, 8), 0, s>>>(n, a, lda);
+  mirror_kernel<T><<<dim3(t, t), dim3(TILE, 8), 0, s>>>(n, a, lda); note_launches();
 }
 
 template <typename T>
 void copy_matrix(int m, int n, const T* a, int lda, T* b, int ldb, cudaStream_t s) {
   if (m <= 0 || n <= 0) return;
-  copy_kernel<T><<<grid_for((size_t)m * n), 256, 0, s>>>(m, n, a, lda, b, ldb);
+  copy_kernel<T><<<grid_for((size_t)m * n), 256, 0, s>>>(m, n, a, lda, b, ldb); note_launches();
 }
 
 template <typename T>
 void set_identity(int n, T* a, int lda, cudaStream_t s) {
   if (n <= 0) return;
-  identity_kernel<T><<<grid_for((size_t)n * n), 256, 0, s>>>(n, a, lda);
+  identity_kernel<T><<<grid_for((size_t)n * n), 256, 0, s>>>(n, a, lda); note_launches();
 }
 
 template <typename T>
 void zero_strict_lower(int n, T* a, int lda, cudaStream_t s) {
   if (n <= 0) return;
-  zero_lower_kernel<T><<<grid_for((size_t)n * n), 256, 0, s>>>(n, a, lda);
+  zero_lower_kernel<T><<<grid_for((size_t)n * n), 256, 0, s>>>(n, a, lda); note_launches();
 }
 
 void convert_f32_to_f64(size_t count, const float* src, double* dst, cudaStream_t s) {
-  if (count) convert_kernel<float, double><<<grid_for(count), 256, 0, s>>>(count, src, dst);
+  if (count) {
+    convert_kernel<float, double><<<grid_for(count), 256, 0, s>>>(count, src, dst);
+    note_launches();
+  }
 }
 void convert_f64_to_f32(size_t count, const double* src, float* dst, cudaStream_t s) {
-  if (count) convert_kernel<double, float><<<grid_for(count), 256, 0, s>>>(count, src, dst);
+  if (count) {
+    convert_kernel<double, float><<<grid_for(count), 256, 0, s>>>(count, src, dst);
+    note_launches();
+  }
 }
 void convert_mat_f32_to_f64(int m, int n, const float* a, int lda, double* b, int ldb, cudaStream_t s) {
-  if (m > 0 && n > 0) convert_mat_kernel<float, double><<<grid_for((size_t)m * n), 256, 0, s>>>(m, n, a, lda, b, ldb);
+  if (m > 0 && n > 0) {
+    convert_mat_kernel<float, double><<<grid_for((size_t)m * n), 256, 0, s>>>(m, n, a, lda, b, ldb);
+    note_launches();
+  }
 }
 void convert_mat_f64_to_f32(int m, int n, const double* a, int lda, float* b, int ldb, cudaStream_t s) {
-  if (m > 0 && n > 0) convert_mat_kernel<double, float><<<grid_for((size_t)m * n), 256, 0, s>>>(m, n, a, lda, b, ldb);
+  if (m > 0 && n > 0) {
+    convert_mat_kernel<double, float><<<grid_for((size_t)m * n), 256, 0, s>>>(m, n, a, lda, b, ldb);
+    note_launches();
+  }
 }
 
 template void symmetrize_upper<double>(int, const double*, int, double*, int, cudaStream_t);

@@ -46,6 +46,11 @@ def lib():
         _lib.xtb_dsygvd_density_adjoint.argtypes = [_I, _P, _I, _P, _I, C.c_double, C.c_double, _P, _I, _P, _I, _P,
                                                     _I, _P, _P, _I]
         _lib.xtb_dsygvd_batched.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P]
+        _lib.xtb_gpu_stage_name.restype = C.c_char_p
+        _lib.xtb_gpu_stage_name.argtypes = [_I]
+        _lib.xtb_gpu_stage_ms.restype = C.c_double
+        _lib.xtb_gpu_stage_ms.argtypes = [_I]
+        _lib.xtb_gpu_launch_count.restype = C.c_longlong
     return _lib
 
 
@@ -93,6 +98,23 @@ def set_option(name: str, value: int) -> None:
 
 def get_option(name: str) -> int:
     return int(lib().xtb_gpu_get_option(name.encode()))
+
+
+def set_device(device: int) -> None:
+    """Select the CUDA device of this thread's later library calls."""
+    if lib().xtb_gpu_set_device(int(device)) != 0:
+        raise GPUError(last_error())
+
+
+def stage_times():
+    """[(stage, ms)] of the calling thread's last call (with set_option("stage_timing", 1))."""
+    L = lib()
+    return [(L.xtb_gpu_stage_name(i).decode(), float(L.xtb_gpu_stage_ms(i))) for i in range(L.xtb_gpu_stage_count())]
+
+
+def launch_count() -> int:
+    """Kernel launches the library has issued so far."""
+    return int(lib().xtb_gpu_launch_count())
 
 
 # ---------------------------------------------------------------------------------------------- xtb sytrd.c ABI
