@@ -74,6 +74,19 @@ void xtb_dsygvd_gpu(const int* itype, const char* jobz, const char* uplo, const 
 int xtb_dsyevd_device(int n, double* a, int lda, double* w, void* stream);
 int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, void* stream);
 
+/* No counterpart in the reference.  dsytrd('U') of a (n x n, lda) in DEVICE memory, in place, with d, e, tau in
+ * device memory, for callers that cannot let a library allocate device memory (they manage every byte on the GPU
+ * through their own pool or allocator, and a cudaMalloc/cudaFree inside a library call would break their budget
+ * and may synchronise the device).  The call allocates nothing: its scratch is a static device array of about
+ * 57 KB that the library holds on every GPU it is loaded on.  Limits: 1 <= n <= XTB_NOALLOC_MAX_N (larger n
+ * returns -1), lda >= n (else -3), and the device must hold the resident rows in shared memory (else -4; B200 does
+ * for every n up to the maximum).  The first call on a device looks up the array's device address, so make it
+ * before any stream capture.  Calls share the array: never let two calls overlap on the GPU.  Work is queued on
+ * `stream` (NULL: the legacy default stream) and the call synchronises it before returning 0, -1000 - cudaError,
+ * or -2000 - device status code (e.g. a device wait that ran past its time limit). */
+#define XTB_NOALLOC_MAX_N 1792
+int xtb_dsytrd_upper_noalloc(int n, double* a, int lda, double* d, double* e, double* tau, void* stream);
+
 /* A batch of independent generalized problems (host arrays, itype 1, jobz 'V', uplo 'U'): problem i has size n[i],
  * a[i] (lda[i]), b[i] (ldb[i]), w[i]; info[i] per problem.  Problems are ordered by n^3 (longest first) and spread
  * over the library's streams.  Returns 0 or the first nonzero info. */

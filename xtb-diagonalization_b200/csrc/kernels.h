@@ -44,6 +44,8 @@ template <typename T>
 SytrdPlan sytrd_plan(int n, int num_sms, size_t max_smem, int grid_override);
 template <typename T>
 cudaError_t sytrd_launch(const SytrdParams<T>& p, const SytrdPlan& pl, cudaStream_t s);
+// Variant reading the upper triangle of p.afull == p.aout in place (FP64, rows in shared memory, n <= 2048).
+cudaError_t sytrd_launch_upper_inplace(const SytrdParams<double>& p, const SytrdPlan& pl, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- utilities
 // dst(0:n,0:n) = symmetric matrix whose upper triangle is src's (src's strict lower triangle is not read).

@@ -30,7 +30,9 @@ constexpr int kRowChunk = 8;  // rows whose partial dot products are reduced tog
 template <typename T>
 __device__ __forceinline__ T ld_cg(const T* p) { return __ldcg(p); }
 
-template <typename T, int NT, int CPT>
+// kUpperInPlace: the variant that reads the upper triangle of p.afull (== p.aout) in place instead of a full
+// symmetric copy, and therefore waits at one extra grid barrier after loading, before any CTA writes the matrix.
+template <typename T, int NT, int CPT, bool kUpperInPlace = false>
 __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p) {
   constexpr int NW = NT / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -58,7 +60,11 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
     if (r >= n) break;
     const T* src = p.afull + (size_t)r * p.ldf;
     T* dst = rows + q * ldr;
-    for (int c = tid; c < n; c += NT) dst[c] = src[c];
+    if constexpr (kUpperInPlace) {
+      for (int c = tid; c < n; c += NT) dst[c] = c <= r ? src[c] : p.afull[r + (size_t)c * p.ldf];
+    } else {
+      for (int c = tid; c < n; c += NT) dst[c] = src[c];
+    }
   }
 
   T x[CPT], vn[CPT], vk[CPT], wk[CPT];
@@ -77,6 +83,9 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
 
   unsigned epoch = 0;
   int par = 0;
+  if constexpr (kUpperInPlace) {
+    if (!group_barrier(p.counter, (unsigned)G, epoch, p.st, p.limit_ns)) return;
+  }
   for (int k = n - 1; k >= 1; --k) {
     const bool has_prev = (k < n - 1);
     // ---- 1. Householder vector from x = A(0:k-1, k); alpha = x(k-1).
@@ -215,7 +224,27 @@ cudaError_t launch_one(const SytrdParams<T>& p, int G, size_t smem, cudaStream_t
   return cudaLaunchCooperativeKernel((void*)kern, dim3(G), dim3(NT), args, smem, s);
 }
 
+template <int CPT>
+cudaError_t launch_upper_inplace(const SytrdParams<double>& p, int G, size_t smem, cudaStream_t s) {
+  auto kern = sytrd_resident_kernel<double, 512, CPT, true>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  void* args[] = {(void*)&p};
+  return cudaLaunchCooperativeKernel((void*)kern, dim3(G), dim3(512), args, smem, s);
+}
+
 }  // namespace
+
+// The in-place variant (upper triangle read where it lies; rows in shared memory; FP64; n <= 2048).
+cudaError_t sytrd_launch_upper_inplace(const SytrdParams<double>& p, const SytrdPlan& pl, cudaStream_t s) {
+  if (p.n <= 0) return cudaSuccess;
+  if (!pl.rows_in_smem || pl.threads != 512) return cudaErrorInvalidValue;
+  switch (pl.cpt) {
+    case 2: return launch_upper_inplace<2>(p, pl.grid, pl.smem, s);
+    case 4: return launch_upper_inplace<4>(p, pl.grid, pl.smem, s);
+  }
+  return cudaErrorInvalidValue;
+}
 
 template <typename T>
 size_t sytrd_smem_bytes(int n, int G, int NT, bool rows_in_smem, int* R_out, int* ldr_out) {
