@@ -103,7 +103,9 @@ int xtb_dsygvd_density_adjoint(int n, const double* h, int ldh, const double* s,
 
 /* Options (process-wide): "sytrd_grid" (CTAs of the resident reduction, 0 = auto), "ormtr_nb" (reflectors per
  * compact-WY block, default 128), "wait_limit_ms" (device wait time limit, default 2000), "stage_timing" (1: record
- * CUDA events at stage boundaries; read with xtb_gpu_stage_*).  Returns 0, or -1 for an unknown name. */
+ * CUDA events at stage boundaries; read with xtb_gpu_stage_*), "graphs" (default 1: a device-pointer solve repeated
+ * on the same buffers and non-NULL stream is captured into a CUDA graph on its second call and replayed after).
+ * Returns 0, or -1 for an unknown name. */
 int xtb_gpu_set_option(const char* name, long value);
 long xtb_gpu_get_option(const char* name);
 

@@ -129,3 +129,39 @@ def test_batched_uneven(xe):
     for (h, s, lam), wi, ci in zip(probs, w, c):
         assert np.max(np.abs(wi - lam)) < 1e-10
         assert metrics.backward_error(h, s, wi, ci) < 10
+
+
+@pytest.mark.parametrize("graphs", [0, 1])
+def test_device_api_repeated_calls_graph_replay(xe, graphs):
+    """Device-pointer solves repeated on the same buffers: eager first call, captured second, replayed after; every
+    call must give the host entry point's result, bit for bit the same across calls."""
+    import torch
+
+    n = 300
+    h, s, lam = inputs.generalized(n, seed=77)
+    w_ref, c_ref, u_ref, info = xe.dsygvd(h, s)
+    assert info == 0
+    dev = torch.device("cuda", 0)
+    xe.set_device(0)
+    stream = torch.cuda.Stream(dev)
+    H0 = torch.from_numpy(np.ascontiguousarray(h)).to(dev)
+    S0 = torch.from_numpy(np.ascontiguousarray(s)).to(dev)
+    H, S = torch.empty_like(H0), torch.empty_like(S0)
+    W = torch.empty(n, dtype=torch.float64, device=dev)
+    old = xe.get_option("graphs")
+    xe.set_option("graphs", graphs)
+    try:
+        outs = []
+        with torch.cuda.stream(stream):
+            for _ in range(4):
+                H.copy_(H0)
+                S.copy_(S0)
+                assert xe.dsygvd_device(n, H.data_ptr(), n, S.data_ptr(), n, W.data_ptr(), stream.cuda_stream) == 0
+                outs.append((W.cpu().numpy().copy(), H.cpu().numpy().T.copy()))
+    finally:
+        xe.set_option("graphs", old)
+    for w, c in outs:
+        np.testing.assert_array_equal(w, outs[0][0])
+        np.testing.assert_array_equal(c, outs[0][1])
+    np.testing.assert_allclose(outs[0][0], w_ref, rtol=0, atol=1e-12)
+    assert metrics.density_error(outs[0][1], c_ref, metrics.aufbau(n, n // 2)) < 1e-9

@@ -26,6 +26,7 @@ std::atomic<long> g_sytrd_grid{0};
 std::atomic<long> g_ormtr_nb{128};
 std::atomic<long> g_wait_ms{2000};
 std::atomic<long> g_stage_timing{0};
+std::atomic<long> g_graphs{1};
 std::atomic<long long> g_launches{0};
 
 struct Buf {
@@ -43,6 +44,18 @@ struct Context {
   DeviceStatus* d_status = nullptr;
   DeviceStatus* h_status = nullptr;
   std::vector<cudaEvent_t> events;  // pool for stage timing
+  // Bumped whenever a buffer is reallocated: captured graphs hold raw buffer addresses and are only replayed while
+  // the generation they were captured in is current.
+  uint64_t generation = 0;
+  std::map<int, bool> stedc_plan_ready;  // per n: the plan buffer "stedc.plan.<n>" holds this n's plan
+  struct GraphEntry {
+    int calls = 0;
+    bool failed = false;
+    uint64_t generation = 0;
+    long long kernels = 0;  // kernel launches captured in the graph (counted again at every replay)
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::map<std::vector<long long>, GraphEntry> graphs;
 };
 
 struct ThreadState {
@@ -105,9 +118,11 @@ struct Call {
 
   // Host-pointer calls run on the context's own stream; device-pointer calls on the caller's stream, where NULL is the
   // CUDA legacy default stream (ordered with the caller's other work on blocking streams).
-  Call(Context* ctx, cudaStream_t user, bool caller_stream = false)
+  // replay: the work (status reset included) comes from a captured graph; nothing is queued here.
+  Call(Context* ctx, cudaStream_t user, bool caller_stream = false, bool replay = false)
       : c(ctx), s(caller_stream ? user : ctx->stream) {
     c->arena.reset();
+    if (replay) return;
     timing = g_stage_timing.load() != 0;
     check(cudaMemsetAsync(c->d_status, 0, sizeof(DeviceStatus), s), "status reset");
     mark("begin");
@@ -142,6 +157,7 @@ struct Call {
         cudaFree(b.p);
         b.p = nullptr;
         b.bytes = 0;
+        c->generation++;
       }
       const size_t grow = bytes + bytes / 8 + 4096;
       if (!check(cudaMalloc(&b.p, grow), key)) return nullptr;
@@ -232,8 +248,7 @@ void stage_sytrd(Call& k, int n, const T* dfull, int ldf, T* dout, int lda, T* d
   T* xch = k.template dev<T>("sytrd.xch", 4 * (size_t)n);
   unsigned* ctr = k.template dev<unsigned>("sytrd.ctr", 64);
   if (!k.ok()) return;
-  p.ybuf = xch;
-  p.cbuf = xch + 2 * (size_t)n;
+  p.xch = xch;
   p.counter = ctr;
   p.st = k.c->d_status;
   p.rows_per_cta = pl.rows_per_cta;
@@ -244,8 +259,7 @@ void stage_sytrd(Call& k, int n, const T* dfull, int ldf, T* dout, int lda, T* d
     p.grows = k.template dev<T>("sytrd.rows", (size_t)pl.grid * pl.rows_per_cta * pl.ldr);
     if (!k.ok()) return;
   }
-  k.check(cudaMemsetAsync(ctr, 0, 64 * sizeof(unsigned), k.s), "sytrd counter");
-  if (k.ok()) k.check(sytrd_launch<T>(p, pl, k.s), "sytrd launch");
+  k.check(cudaMemsetAsync(ctr, 0, 64 * sizeof(unsigned), k.s), "sytrd counter");  if (k.ok()) k.check(sytrd_launch<T>(p, pl, k.s), "sytrd launch");
 }
 
 template <typename T>
@@ -261,10 +275,17 @@ void stage_stedc(Call& k, int n, double* d, double* e, double* z, int ldz) {
   if (!k.ok() || n <= 0) return;
   const size_t wb = stedc_work_bytes(n);
   char* w = k.template dev<char>("stedc.work", wb);
+  const std::string plan_key = "stedc.plan." + std::to_string(n);
+  const size_t pb = stedc_plan_bytes(n);
+  bool& ready = k.c->stedc_plan_ready[n];
+  const bool fresh = k.c->dbufs.find(plan_key) == k.c->dbufs.end();
+  char* plan = k.template dev<char>(plan_key.c_str(), pb);
+  if (fresh) ready = false;
   const size_t hb = (size_t)40 * n * sizeof(int) + (size_t)4 * (n + 8) * sizeof(GemmDesc<double>) + 4096;
-  char* h = k.template host<char>("stedc.stage", hb);
+  char* h = ready ? nullptr : k.template host<char>("stedc.stage", hb);
   if (!k.ok()) return;
-  k.check(stedc_device(n, d, e, z, ldz, w, wb, h, hb, k.c->d_status, k.s), "stedc");
+  k.check(stedc_device(n, d, e, z, ldz, w, wb, plan, !ready, h, hb, k.c->d_status, k.s), "stedc");
+  if (k.ok()) ready = true;
 }
 
 // The generalized core on device buffers: h (n x n, full symmetric, ld n) is consumed; u (n x n, ld n) holds B's upper
@@ -279,10 +300,8 @@ void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
   double* e = k.template dev<double>("gv.e", (size_t)n);
   double* tau = k.template dev<double>("gv.tau", (size_t)n);
   if (!k.ok()) return;
-  k.check(potrf_upper(n, u, n, k.c->d_status, k.c->arena, k.s), "potrf");
-  k.mark("potrf");
-  if (k.ok()) k.check(trtri_upper(n, u, n, x, n, t, k.c->arena, k.s), "trtri");
-  k.mark("trtri");
+  k.check(potrf_inverse_upper(n, u, n, x, n, t, k.c->d_status, k.c->arena, k.s), "potrf+inverse");
+  k.mark("potrf_inverse");
   // G = H X (X upper), then H' = X^T G on the upper tiles, symmetrised for the reduction.
   GemmDesc<double> p = gemm_problem<double>(n, n, n, 1.0, h, n, 0, x, n, 0, 0.0, t, n, kTriBUpper);
   if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "congruence 1");
@@ -432,6 +451,66 @@ void stedc_host(const int* n_, T* d, T* e, T* z, const int* ldz_, T* work, const
   DeviceStatus st{};
   const int code = k.finish(&st);
   *info = info_of(code, st, n);
+}
+
+// Repeated device-pointer solves on the same buffers and stream: the first call runs eagerly (it allocates the
+// workspace and uploads per-size plans), the second is captured into a CUDA graph while it runs, later calls replay
+// the graph (one launch instead of a few hundred).  A graph is dropped when any workspace buffer was reallocated
+// since its capture; capture failures fall back to eager execution for that key.  Calls on the legacy default
+// stream (NULL) and calls with stage timing on always run eagerly.
+template <typename Body>
+int run_graphed(Context* c, cudaStream_t s, const std::vector<long long>& key, DeviceStatus* st_out, Body body) {
+  Context::GraphEntry& ge = c->graphs[key];
+  const bool graphs_on = g_graphs.load() != 0 && g_stage_timing.load() == 0 && s != nullptr;
+  if (graphs_on && ge.exec && ge.generation == c->generation) {
+    Call k(c, s, true, true);
+    k.check(cudaGraphLaunch(ge.exec, s), "graph launch");
+    g_launches.fetch_add(ge.kernels, std::memory_order_relaxed);
+    ge.calls++;
+    return k.finish(st_out);
+  }
+  if (ge.exec) {
+    cudaGraphExecDestroy(ge.exec);
+    ge.exec = nullptr;
+  }
+  if (graphs_on && ge.calls >= 1 && !ge.failed) {
+    const uint64_t gen0 = c->generation;
+    const long long launches0 = g_launches.load();
+    cudaError_t err = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (err == cudaSuccess) {
+      {
+        Call k(c, s, true);
+        body(k);
+        err = k.err;
+      }
+      // Captured launches are not executed now: move them from the counter to the entry's per-replay count.
+      ge.kernels = g_launches.load() - launches0;
+      g_launches.fetch_sub(ge.kernels, std::memory_order_relaxed);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+      if (err == cudaSuccess && e2 == cudaSuccess && graph && c->generation == gen0) {
+        cudaGraphExec_t exec = nullptr;
+        if (cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+          ge.exec = exec;
+          ge.generation = gen0;
+        }
+      }
+      if (graph) cudaGraphDestroy(graph);
+    }
+    (void)cudaGetLastError();  // a capture that failed leaves no sticky error behind
+    if (ge.exec) {
+      Call k(c, s, true, true);
+      k.check(cudaGraphLaunch(ge.exec, s), "graph launch");
+      g_launches.fetch_add(ge.kernels, std::memory_order_relaxed);
+      ge.calls++;
+      return k.finish(st_out);
+    }
+    ge.failed = true;
+  }
+  Call k(c, s, true);
+  body(k);
+  ge.calls++;
+  return k.finish(st_out);
 }
 
 }  // namespace
@@ -600,14 +679,16 @@ int xtb_dsyevd_device(int n, double* a, int lda, double* w, void* stream) {
   if (n == 0) return 0;
   Context* c = context();
   if (!c) return t_state.last_code;
-  Call k(c, (cudaStream_t)stream, true);
-  double* df = k.dev<double>("dv.F", (size_t)n * n);
-  double* dz = k.dev<double>("dv.Z", (size_t)n * n);
-  if (k.ok()) symmetrize_upper<double>(n, a, lda, df, n, k.s);
-  core_syevd(k, n, df, dz, w, true);
-  if (k.ok()) copy_matrix<double>(n, n, dz, n, a, lda, k.s);
+  const std::vector<long long> key = {2, n, (long long)(uintptr_t)a, lda, (long long)(uintptr_t)w,
+                                      (long long)(uintptr_t)stream};
   DeviceStatus st{};
-  const int code = k.finish(&st);
+  const int code = run_graphed(c, (cudaStream_t)stream, key, &st, [&](Call& k) {
+    double* df = k.dev<double>("dv.F", (size_t)n * n);
+    double* dz = k.dev<double>("dv.Z", (size_t)n * n);
+    if (k.ok()) symmetrize_upper<double>(n, a, lda, df, n, k.s);
+    core_syevd(k, n, df, dz, w, true);
+    if (k.ok()) copy_matrix<double>(n, n, dz, n, a, lda, k.s);
+  });
   return info_of(code, st, n);
 }
 
@@ -618,21 +699,23 @@ int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, 
   if (n == 0) return 0;
   Context* c = context();
   if (!c) return t_state.last_code;
-  Call k(c, (cudaStream_t)stream, true);
-  double* dh = k.dev<double>("dv.F", (size_t)n * n);
-  double* du = k.dev<double>("dv.U", (size_t)n * n);
-  double* dc = k.dev<double>("dv.C", (size_t)n * n);
-  if (k.ok()) {
-    symmetrize_upper<double>(n, a, lda, dh, n, k.s);
-    copy_matrix<double>(n, n, b, ldb, du, n, k.s);
-  }
-  core_sygvd(k, n, dh, du, dc, w);
-  if (k.ok()) {
-    copy_matrix<double>(n, n, dc, n, a, lda, k.s);
-    copy_matrix<double>(n, n, du, n, b, ldb, k.s);
-  }
+  const std::vector<long long> key = {1, n, (long long)(uintptr_t)a, lda, (long long)(uintptr_t)b, ldb,
+                                      (long long)(uintptr_t)w, (long long)(uintptr_t)stream};
   DeviceStatus st{};
-  const int code = k.finish(&st);
+  const int code = run_graphed(c, (cudaStream_t)stream, key, &st, [&](Call& k) {
+    double* dh = k.dev<double>("dv.F", (size_t)n * n);
+    double* du = k.dev<double>("dv.U", (size_t)n * n);
+    double* dc = k.dev<double>("dv.C", (size_t)n * n);
+    if (k.ok()) {
+      symmetrize_upper<double>(n, a, lda, dh, n, k.s);
+      copy_matrix<double>(n, n, b, ldb, du, n, k.s);
+    }
+    core_sygvd(k, n, dh, du, dc, w);
+    if (k.ok()) {
+      copy_matrix<double>(n, n, dc, n, a, lda, k.s);
+      copy_matrix<double>(n, n, du, n, b, ldb, k.s);
+    }
+  });
   return info_of(code, st, n);
 }
 
@@ -717,6 +800,7 @@ int xtb_gpu_set_option(const char* name, long value) {
   if (!std::strcmp(name, "ormtr_nb")) { g_ormtr_nb = value; return 0; }
   if (!std::strcmp(name, "wait_limit_ms")) { g_wait_ms = value; return 0; }
   if (!std::strcmp(name, "stage_timing")) { g_stage_timing = value; return 0; }
+  if (!std::strcmp(name, "graphs")) { g_graphs = value; return 0; }
   return -1;
 }
 
@@ -726,6 +810,7 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "ormtr_nb")) return g_ormtr_nb;
   if (!std::strcmp(name, "wait_limit_ms")) return g_wait_ms;
   if (!std::strcmp(name, "stage_timing")) return g_stage_timing;
+  if (!std::strcmp(name, "graphs")) return g_graphs;
   return -1;
 }
 

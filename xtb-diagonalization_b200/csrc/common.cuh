@@ -52,6 +52,9 @@ __device__ __forceinline__ int ld_volatile_i32(const int* p) { return *(const vo
 
 // Barrier among `members` CTAs sharing one monotonically increasing counter (zeroed before the launch).
 // Each call advances the caller's `epoch`; the barrier completes when the counter reaches epoch * members.
+// Ordering: the CTA's writes before the call are ordered before thread 0's release-add by the __syncthreads, and the
+// acquire load that sees the final count is ordered before every thread's later reads by the second __syncthreads,
+// so no separate fence is needed (each fence would cost an extra round trip on the critical path).
 // Returns false (and records kStatusBarrierTimeout) if the wait exceeds `limit_ns`, or if another CTA already
 // recorded an error; callers then leave the kernel.  Must be called by all threads of the CTA.
 __device__ __forceinline__ bool group_barrier(unsigned* counter, unsigned members, unsigned& epoch,
@@ -61,7 +64,6 @@ __device__ __forceinline__ bool group_barrier(unsigned* counter, unsigned member
   epoch += 1;
   if (threadIdx.x == 0) {
     int ok = 1;
-    __threadfence();
     red_release_add_u32(counter, 1u);
     const unsigned target = epoch * members;
     uint64_t t0 = 0;
@@ -78,7 +80,6 @@ __device__ __forceinline__ bool group_barrier(unsigned* counter, unsigned member
         }
       }
     }
-    __threadfence();
     s_ok = ok;
   }
   __syncthreads();

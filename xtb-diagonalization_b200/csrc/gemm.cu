@@ -1,5 +1,5 @@
 // Grouped GEMM kernel (see gemm.cuh).  64 x 64 output tile per CTA, 4 warps each owning 32 x 32, K in steps of 16
-// staged through shared memory by cp.async (two stages).  For FP64 every warp issues mma.sync.m8n8k4 f64: per
+// staged through shared memory by a four-stage cp.async pipeline.  For FP64 every warp issues mma.sync.m8n8k4 f64: per
 // k-step of 4 a thread loads one A and one B element per 8 x 8 sub-tile (layout of the PTX ISA's m8n8k4 .f64 shape:
 // A row = lane/4, col = lane%4; B row = lane%4, col = lane/4; C row = lane/4, cols 2*(lane%4) + {0,1}).
 #include "gemm.cuh"
@@ -126,23 +126,47 @@ struct Frag<float> {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(kGemmThreads) gemm_grouped_kernel(const GemmDesc<T>* __restrict__ descs,
-                                                                     int nprob) {
-  __shared__ __align__(16) T As[2][BK * SA];
-  __shared__ __align__(16) T Bs[2][BK * SB];
+struct DescFromMemory {
+  const GemmDesc<T>* d;
+  int n;
+  __device__ const GemmDesc<T>& get(int i) const { return d[i]; }
+};
+
+// Up to kGemmInlineMax descriptors passed by value in the kernel's parameter space: no host-to-device copy is queued
+// ahead of the launch (a copy per small GEMM would serialise behind the stream and dominate short GEMMs).
+template <typename T>
+struct DescInline {
+  GemmDesc<T> d[kGemmInlineMax];
+  int n;
+  __device__ const GemmDesc<T>& get(int i) const { return d[i]; }
+};
+
+// Stages of the cp.async pipeline: three K-tiles in flight while one is consumed hides the L2/HBM latency behind the
+// DMMA loop (two stages left the tensor pipe waiting on loads).
+constexpr int STAGES = 4;
+template <typename T>
+constexpr size_t gemm_smem_bytes() {
+  return (size_t)STAGES * (BK * SA + BK * SB) * sizeof(T);
+}
+
+template <typename T, typename Src>
+__global__ void __launch_bounds__(kGemmThreads) gemm_grouped_kernel(const __grid_constant__ Src src) {
+  extern __shared__ __align__(16) unsigned char gemm_smem[];
+  T* As = reinterpret_cast<T*>(gemm_smem);  // [STAGES][BK * SA]
+  T* Bs = As + STAGES * BK * SA;             // [STAGES][BK * SB]
   __shared__ int s_prob;
 
   const int tile = blockIdx.x;
   if (threadIdx.x == 0) {
-    int lo = 0, hi = nprob - 1;
+    int lo = 0, hi = src.n - 1;
     while (lo < hi) {  // last problem whose tile_begin <= tile
       int mid = (lo + hi + 1) >> 1;
-      if (descs[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+      if (src.get(mid).tile_begin <= tile) lo = mid; else hi = mid - 1;
     }
     s_prob = lo;
   }
   __syncthreads();
-  const GemmDesc<T> p = descs[s_prob];
+  const GemmDesc<T> p = src.get(s_prob);
   const int local = tile - p.tile_begin;
   if (local < 0 || local >= p.tiles_m * p.tiles_n) return;
   const int tm = local % p.tiles_m, tn = local / p.tiles_m;
@@ -168,21 +192,24 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_grouped_kernel(const GemmDe
 
   const int nk = khi > klo ? (khi - klo + BK - 1) / BK : 0;
   if (nk > 0) {
-    load_tiles<T>(p, As[0], Bs[0], m0, n0, klo);
-    cp_async_commit();
-    for (int it = 0; it < nk; ++it) {
-      const int cur = it & 1;
-      if (it + 1 < nk) {
-        load_tiles<T>(p, As[cur ^ 1], Bs[cur ^ 1], m0, n0, klo + (it + 1) * BK);
-        cp_async_commit();
-        cp_async_wait<1>();
-      } else {
-        cp_async_wait<0>();
-      }
-      __syncthreads();
 #pragma unroll
-      for (int kk = 0; kk < BK / 4; ++kk) Frag<T>::step(acc, As[cur], Bs[cur], kk, wm, wn, lane);
-      __syncthreads();
+    for (int st = 0; st < STAGES - 1; ++st) {
+      if (st < nk) load_tiles<T>(p, As + st * BK * SA, Bs + st * BK * SB, m0, n0, klo + st * BK);
+      cp_async_commit();
+    }
+    for (int it = 0; it < nk; ++it) {
+      cp_async_wait<STAGES - 2>();  // K-tile `it` has landed
+      __syncthreads();              // ... for every thread, and K-tile it-1's buffer is free
+      const int pf = it + STAGES - 1;
+      if (pf < nk) {
+        const int b = pf % STAGES;
+        load_tiles<T>(p, As + b * BK * SA, Bs + b * BK * SB, m0, n0, klo + pf * BK);
+      }
+      cp_async_commit();
+      const int cur = it % STAGES;
+#pragma unroll
+      for (int kk = 0; kk < BK / 4; ++kk)
+        Frag<T>::step(acc, As + cur * BK * SA, Bs + cur * BK * SB, kk, wm, wn, lane);
     }
   }
 
@@ -209,12 +236,29 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_grouped_kernel(const GemmDe
   }
 }
 
+// The pipeline's shared memory exceeds the default 48 KB: opt in once per device and kernel instantiation.
+template <typename T, typename Src>
+cudaError_t gemm_enable_smem() {
+  static bool enabled[64];
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  if (dev >= 0 && dev < 64 && enabled[dev]) return cudaSuccess;
+  err = cudaFuncSetAttribute(gemm_grouped_kernel<T, Src>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)gemm_smem_bytes<T>());
+  if (err == cudaSuccess && dev >= 0 && dev < 64) enabled[dev] = true;
+  return err;
+}
+
 }  // namespace
 
 template <typename T>
 void gemm_grouped_launch(const GemmDesc<T>* d_descs, int nprob, int total_tiles, cudaStream_t s) {
   if (nprob <= 0 || total_tiles <= 0) return;
-  gemm_grouped_kernel<T><<<total_tiles, kGemmThreads, 0, s>>>(d_descs, nprob); note_launches();
+  DescFromMemory<T> src{d_descs, nprob};
+  if (gemm_enable_smem<T, DescFromMemory<T>>() != cudaSuccess) return;
+  gemm_grouped_kernel<T, DescFromMemory<T>><<<total_tiles, kGemmThreads, gemm_smem_bytes<T>(), s>>>(src);
+  note_launches();
 }
 
 template void gemm_grouped_launch<double>(const GemmDesc<double>*, int, int, cudaStream_t);
@@ -236,10 +280,12 @@ GemmDesc<T> gemm_problem(int M, int N, int K, T alpha, const T* A, int lda, int 
 template <typename T>
 cudaError_t gemm_group(DescArena& arena, const GemmDesc<T>* probs, int nprob, cudaStream_t s) {
   if (nprob <= 0) return cudaSuccess;
-  char* h;
-  char* d;
-  if (!arena.take((size_t)nprob * sizeof(GemmDesc<T>), &h, &d)) return cudaErrorMemoryAllocation;
-  GemmDesc<T>* hd = reinterpret_cast<GemmDesc<T>*>(h);
+  char* h = nullptr;
+  char* d = nullptr;
+  DescInline<T> inl;
+  const bool inline_descs = nprob <= kGemmInlineMax;
+  if (!inline_descs && !arena.take((size_t)nprob * sizeof(GemmDesc<T>), &h, &d)) return cudaErrorMemoryAllocation;
+  GemmDesc<T>* hd = inline_descs ? inl.d : reinterpret_cast<GemmDesc<T>*>(h);
   int tb = 0;
   for (int i = 0; i < nprob; ++i) {
     hd[i] = probs[i];
@@ -250,6 +296,14 @@ cudaError_t gemm_group(DescArena& arena, const GemmDesc<T>* probs, int nprob, cu
     tb += hd[i].tiles_m * hd[i].tiles_n;
   }
   if (tb == 0) return cudaSuccess;
+  if (inline_descs) {
+    inl.n = nprob;
+    cudaError_t e = gemm_enable_smem<T, DescInline<T>>();
+    if (e != cudaSuccess) return e;
+    gemm_grouped_kernel<T, DescInline<T>><<<tb, kGemmThreads, gemm_smem_bytes<T>(), s>>>(inl);
+    note_launches();
+    return cudaGetLastError();
+  }
   cudaError_t err = cudaMemcpyAsync(d, h, (size_t)nprob * sizeof(GemmDesc<T>), cudaMemcpyHostToDevice, s);
   if (err != cudaSuccess) return err;
   gemm_grouped_launch<T>(reinterpret_cast<GemmDesc<T>*>(d), nprob, tb, s);

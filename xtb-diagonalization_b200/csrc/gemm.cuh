@@ -43,6 +43,7 @@ struct GemmDesc {
 };
 
 constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 16, kGemmThreads = 128;
+constexpr int kGemmInlineMax = 32;  // descriptors passed by value in the launch (parameter space)
 
 inline int gemm_tiles(int m, int n) {
   return ((m + kGemmBM - 1) / kGemmBM) * ((n + kGemmBN - 1) / kGemmBN);

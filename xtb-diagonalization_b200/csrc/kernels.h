@@ -23,8 +23,7 @@ struct SytrdParams {
   T* d;
   T* e;
   T* tau;
-  T* ybuf;         // 2 n exchange (y = A v)
-  T* cbuf;         // 2 n exchange (next column)
+  T* xch;          // 2 x n (y_r, A(r,k-1)) pairs, two alternating exchange buffers
   T* grows;        // global row slab when rows do not fit shared memory (grid * rows_per_cta * ldr)
   unsigned* counter;
   DeviceStatus* st;
@@ -113,15 +112,17 @@ struct StedcWork;  // opaque, sized by stedc_work_bytes
 size_t stedc_work_bytes(int n);
 // Eigenpairs of the symmetric tridiagonal (d, e) on the device: d <- eigenvalues ascending, z (n x n, ldz) <-
 // orthonormal eigenvectors.  Returns LAPACK-style info through st (kStatusSecularNoConv).
-cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* work, size_t work_bytes,
-                         void* hstage, size_t hstage_bytes, DeviceStatus* st, cudaStream_t s);
+// `plan` (stedc_plan_bytes(n)) holds the per-level plan for this n; upload_plan copies it from hstage first (needed
+// once per plan buffer).
+size_t stedc_plan_bytes(int n);
+cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* work, size_t work_bytes, void* plan,
+                         bool upload_plan, void* hstage, size_t hstage_bytes, DeviceStatus* st, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- potrf / trtri
-// In-place upper Cholesky of S (n x n, lds); status kStatusNotSPD with info = failing column (1-based).
-cudaError_t potrf_upper(int n, double* a, int lda, DeviceStatus* st, DescArena& arena, cudaStream_t s);
-// X = U^-1 (upper; strict lower part of X set to zero).  tmp: n x n scratch (ld n).
-cudaError_t trtri_upper(int n, const double* u, int ldu, double* x, int ldx, double* tmp, DescArena& arena,
-                        cudaStream_t s);
+// S = U^T U (upper, in place) and X = U^-1 (upper, strict lower part zero) in one recursion; t: n x n scratch (ld n).
+// A non-SPD S records kStatusNotSPD with info = the failing column (1-based).
+cudaError_t potrf_inverse_upper(int n, double* a, int lda, double* x, int ldx, double* t, DeviceStatus* st,
+                                DescArena& arena, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- adjoint
 // Daleckii-Krein gradient of sum(Wbar o C diag(f) C^T): dh, ds (n x n, ld n); t1..t3 n x n scratch.

@@ -76,8 +76,7 @@ extern "C" int xtb_dsytrd_upper_noalloc(int n, double* a, int lda, double* d, do
   p.d = d;
   p.e = e;
   p.tau = tau;
-  p.ybuf = reinterpret_cast<double*>(base + kVectorOffset);
-  p.cbuf = p.ybuf + 2 * (size_t)n;
+  p.xch = reinterpret_cast<double*>(base + kVectorOffset);
   p.counter = reinterpret_cast<unsigned*>(base + kCounterOffset);
   p.st = reinterpret_cast<DeviceStatus*>(base + kStatusOffset);
   p.grows = nullptr;

@@ -68,13 +68,37 @@ __global__ void wy_factor_kernel(int nm1, int nb, const T* __restrict__ tau, T* 
   }
 }
 
+// W = sum over the split-K slices, in slice order (deterministic): parts is S slices of kb x m (ld nb, stride nb*m).
+template <typename T>
+__global__ void splitk_sum_kernel(int kb, int m, int nb, int S, const T* __restrict__ parts, T* __restrict__ w) {
+  const size_t total = (size_t)kb * m;
+  const size_t stride = (size_t)nb * m;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx % kb), c = (int)(idx / kb);
+    const size_t off = r + (size_t)c * nb;
+    T acc = parts[off];
+    for (int sl = 1; sl < S; ++sl) acc += parts[off + sl * stride];
+    w[off] = acc;
+  }
+}
+
+constexpr int kMaxSplit = 8;
+
+// Split-K slices for W = V_b^T Z: enough CTAs to cover the SMs twice, slices of at least 128 rows.
+inline int split_count(int kb, int m, int rows) {
+  const int tiles = ((kb + kGemmBM - 1) / kGemmBM) * ((m + kGemmBN - 1) / kGemmBN);
+  int S = (2 * 148 + tiles - 1) / tiles;
+  S = std::min(S, std::max(1, rows / 128));
+  return std::max(1, std::min(S, kMaxSplit));
+}
+
 }  // namespace
 
 template <typename T>
 size_t ormtr_work_elems(int n, int m, int nb) {
   const size_t nm1 = n > 1 ? (size_t)(n - 1) : 1;
   const size_t nblocks = (nm1 + nb - 1) / nb;
-  return 2 * (size_t)n * nm1 + nblocks * nb * nb + (size_t)nb * (m > 0 ? m : 1) + 4 * 64;
+  return 2 * (size_t)n * nm1 + nblocks * nb * nb + (size_t)(kMaxSplit + 1) * nb * (m > 0 ? m : 1) + 4 * 64;
 }
 
 template <typename T>
@@ -126,11 +150,32 @@ cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, i
   err = gemm_group<T>(arena, probs, nblocks, s);
   delete[] probs;
   if (err != cudaSuccess) return err;
-  // Apply the blocks in increasing order.
+  // Apply the blocks in increasing order.  W = V_b^T Z has only kb (<= nb) rows, so its long K (the block's rows) is
+  // split across slices computed in one grouped launch and summed in slice order.
+  T* parts = w.W + (size_t)nb * m;
   for (int b = 0; b < nblocks; ++b) {
     const int j0 = b * nb, kb = std::min(nb, nm1 - j0), rows = j0 + kb;
-    GemmDesc<T> p1 = gemm_problem<T>(kb, m, rows, T(1), w.V + (size_t)j0 * n, n, 1, z, ldz, 0, T(0), w.W, nb);
-    err = gemm_group<T>(arena, &p1, 1, s);
+    const int S = split_count(kb, m, rows);
+    if (S == 1) {
+      GemmDesc<T> p1 = gemm_problem<T>(kb, m, rows, T(1), w.V + (size_t)j0 * n, n, 1, z, ldz, 0, T(0), w.W, nb);
+      err = gemm_group<T>(arena, &p1, 1, s);
+    } else {
+      GemmDesc<T> ps[kMaxSplit];
+      const int ks = ((rows + S - 1) / S + kGemmBK - 1) / kGemmBK * kGemmBK;
+      int used = 0;
+      for (int sl = 0; sl < S; ++sl) {
+        const int r0 = sl * ks, kr = std::min(ks, rows - r0);
+        if (kr <= 0) break;
+        ps[used++] = gemm_problem<T>(kb, m, kr, T(1), w.V + r0 + (size_t)j0 * n, n, 1, z + r0, ldz, 0, T(0),
+                                     parts + (size_t)sl * nb * m, nb);
+      }
+      err = gemm_group<T>(arena, ps, used, s);
+      if (err == cudaSuccess) {
+        const size_t total = (size_t)kb * m;
+        const int grid = (int)std::min<size_t>((total + 255) / 256, 148 * 8);
+        splitk_sum_kernel<T><<<grid, 256, 0, s>>>(kb, m, nb, used, parts, w.W); note_launches();
+      }
+    }
     if (err != cudaSuccess) return err;
     GemmDesc<T> p2 = gemm_problem<T>(rows, m, kb, T(-1), w.Y + (size_t)j0 * n, n, 0, w.W, nb, 0, T(1), z, ldz);
     err = gemm_group<T>(arena, &p2, 1, s);

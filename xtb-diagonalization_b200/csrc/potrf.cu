@@ -1,17 +1,16 @@
-// Cholesky factor S = U^T U and the explicit inverse X = U^-1 for the generalized problem H C = S C e.
+// Cholesky factor S = U^T U and its explicit inverse X = U^-1 for the generalized problem H C = S C e.
 //
 // xTB factors S once per geometry (mctc_potrf) and reduces every cycle with dsygst or with the congruence
 // H' = X^T H X, X = U^-1 (xtb #1466; reference scripts/kernels/congruence.c:1-52 studies it; EigenBench's dump reader
-// does dpotrf, dtrtri, two dtrmm: Sources/EigenBench/main.swift:167-172).  This file supplies the first two steps;
-// the congruence and the final C = X C' are tensor-core GEMMs with triangular masks.
-//
-// potrf (upper, right-looking, blocks of 64): one CTA factors the FP64 diagonal block in shared memory, one kernel
-// solves the block row (U_jj^-T A_j,:), a grouped tensor-core GEMM applies the trailing update to the upper tiles.
-// A non-positive or NaN pivot records kStatusNotSPD with the global column (1-based), as LAPACK's info.
-// trtri (upper): diagonal blocks inverted in shared memory (one CTA each), then log2(n/64) levels of doubling,
-// X12 = -X11 (U12 X22), every pair of a level in the same two grouped GEMM launches.
+// does dpotrf, dtrtri and two dtrmm: Sources/EigenBench/main.swift:167-172).  Here both factors come out of one
+// recursion:
+//     [A11 A12; . A22]:  (U11, X11) = chol_inv(A11);  U12 = X11^T A12;  A22 -= U12^T U12;
+//                        (U22, X22) = chol_inv(A22);  X12 = -X11 U12 X22,
+// every off-diagonal step a triangular-masked FP64 tensor-core GEMM, the 64 x 64 leaves factored and inverted in
+// shared memory by one CTA (two block syncs per factorization step, one per inverse column).
+// A pivot that is not > 0 (or NaN) records kStatusNotSPD with the global column (1-based), LAPACK's info; the kernels
+// of the remaining recursion then return at once.
 #include <algorithm>
-#include <vector>
 
 #include "kernels.h"
 
@@ -20,152 +19,143 @@ namespace xtbeig {
 namespace {
 
 constexpr int NB = 64;
+constexpr size_t kLeafSmem = (size_t)(2 * NB * (NB + 1) + NB) * sizeof(double);
 
-__global__ void potrf_diag_kernel(int n, double* a, int lda, int j, DeviceStatus* st) {
-  __shared__ double blk[NB][NB + 1];  // blk[col][row]
-  const int nb = min(NB, n - j);
+// One CTA of 256 threads: U (upper Cholesky factor of the nb x nb block at (j0, j0), nb <= 64) in place in `a`,
+// X = U^-1 (upper, zero below the diagonal) into `x`.
+//   factor: per step k every thread forms 1/sqrt(U(k,k)) itself, the row is scaled, and the trailing triangle is
+//           updated by a 16 x 16 thread tile (two block syncs per step);
+//   invert: column by column, X(0:c-1, c) = -X(c,c) X(0:c-1, 0:c-1) U(0:c-1, c), eight threads per row each summing
+//           every eighth term, combined by three shuffles (one block sync per column).
+__global__ void __launch_bounds__(256) chol_inv_leaf_kernel(double* a, int lda, double* x, int ldx, int j0, int nb,
+                                                            DeviceStatus* st) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double(*U)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(smem_raw);
+  double(*X)[NB + 1] = U + NB;
+  double* dinv = reinterpret_cast<double*>(X + NB);
   if (ld_volatile_i32(&st->code) != 0) return;
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int r = idx % nb, c = idx / nb;
-    blk[c][r] = (r <= c) ? a[(j + r) + (size_t)(j + c) * lda] : 0.0;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  for (int idx = tid; idx < NB * NB; idx += 256) {  // the whole 64 x 64 frame: zero outside the nb x nb block
+    const int r = idx % NB, c = idx / NB;
+    U[r][c] = (r <= c && c < nb) ? a[(j0 + r) + (size_t)(j0 + c) * lda] : 0.0;
+    X[r][c] = 0.0;
   }
   __syncthreads();
   for (int k = 0; k < nb; ++k) {
-    const double piv = blk[k][k];
+    const double piv = U[k][k];
     if (!(piv > 0.0)) {
-      if (threadIdx.x == 0) set_status(st, kStatusNotSPD, j + k + 1, 0);
-      return;  // uniform: every thread sees the same pivot
+      if (tid == 0) set_status(st, kStatusNotSPD, j0 + k + 1, 0);
+      return;  // uniform: every thread read the same pivot
     }
-    const double u = sqrt(piv);
+    const double inv = rsqrt(piv), u = piv * inv;  // one reciprocal square root on the step's critical path
+    const int c = k + 1 + tid;
+    if (c < nb) U[k][c] *= inv;
     __syncthreads();
-    // Row k of U: U(k, c) = A(k, c) / u for c >= k.
-    for (int c = k + threadIdx.x; c < nb; c += blockDim.x) blk[c][k] = (c == k) ? u : blk[c][k] / u;
-    __syncthreads();
-    // Trailing: A(r, c) -= U(k, r) U(k, c) for k < r <= c.
-    const int m = nb - k - 1;
-    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
-      const int r = k + 1 + idx % m, c = k + 1 + idx / m;
-      if (r <= c) blk[c][r] -= blk[r][k] * blk[c][k];
+    for (int i = 0; i < 4; ++i) {
+      const int r = k + 1 + ty + 16 * i;
+      if (r >= nb) break;
+      const double ukr = U[k][r];
+      for (int j = 0; j < 4; ++j) {
+        const int cc = k + 1 + tx + 16 * j;
+        if (cc >= r && cc < nb) U[r][cc] -= ukr * U[k][cc];
+      }
+    }
+    if (tid == 0) {
+      U[k][k] = u;  // nobody reads U(k,k) after this step's pivot read
+      dinv[k] = inv;
     }
     __syncthreads();
   }
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+  for (int idx = tid; idx < nb * nb; idx += 256) {
     const int r = idx % nb, c = idx / nb;
-    if (r <= c) a[(j + r) + (size_t)(j + c) * lda] = blk[c][r];
+    if (r <= c) a[(j0 + r) + (size_t)(j0 + c) * lda] = U[r][c];
+  }
+  // Inverse by doubling: the 8 x 8 diagonal blocks by back substitution (one thread per column), then for block
+  // sizes s = 8, 16, 32 every pair of neighbouring inverted blocks is joined: T = U12 X22, X12 = -X11 T.  The
+  // sub-diagonal part of U is zero and padding rows/columns beyond nb act as identity-free zeros, so the joins can
+  // run over the full 64 x 64 frame; only entries < nb are written back.
+  if (tid < NB) {
+    const int c = tid, b0 = (c / 8) * 8;
+    if (c < nb) {
+      X[c][c] = dinv[c];
+      for (int i = c - 1; i >= b0; --i) {
+        double sacc = 0.0;
+        for (int q = i + 1; q <= c; ++q) sacc += U[i][q] * X[q][c];
+        X[i][c] = -dinv[i] * sacc;
+      }
+    }
+  }
+  __syncthreads();
+  for (int sz = 8; sz < NB; sz *= 2) {
+    // T = U12 X22 for every pair (block rows p..p+sz, block cols p+sz..p+2sz), stored in the strict lower part of U
+    // transposed: T(r, c) -> U[c][r] (c > r always, so this area is unused).
+    const int npair = NB / (2 * sz);
+    for (int idx = tid; idx < npair * sz * sz; idx += 256) {
+      const int pr = idx / (sz * sz), rem = idx % (sz * sz);
+      const int r = pr * 2 * sz + rem % sz, c = pr * 2 * sz + sz + rem / sz;
+      double sacc = 0.0;
+      const int q0 = pr * 2 * sz + sz;
+      for (int q = q0; q <= c; ++q) sacc += U[r][q] * X[q][c];
+      U[c][r] = sacc;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < npair * sz * sz; idx += 256) {
+      const int pr = idx / (sz * sz), rem = idx % (sz * sz);
+      const int r = pr * 2 * sz + rem % sz, c = pr * 2 * sz + sz + rem / sz;
+      double sacc = 0.0;
+      const int qe = pr * 2 * sz + sz;
+      for (int q = r; q < qe; ++q) sacc += X[r][q] * U[c][q];
+      X[r][c] = -sacc;
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < nb * nb; idx += 256) {
+    const int r = idx % nb, c = idx / nb;
+    x[(j0 + r) + (size_t)(j0 + c) * ldx] = X[r][c];
   }
 }
 
-// Block row: B = U_jj^-T B for the nb x w panel right of the diagonal block (forward substitution, one thread per
-// column, the column held in shared memory).
-__global__ void potrf_trsm_kernel(int n, double* a, int lda, int j, DeviceStatus* st) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* U = reinterpret_cast<double*>(smem_raw);  // NB x NB, U[c * NB + r]
-  double* X = U + NB * NB;                          // NB x blockDim.x, X[r * blockDim.x + t]
-  if (ld_volatile_i32(&st->code) != 0) return;
-  const int nb = min(NB, n - j);
-  const int c0 = j + nb;
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int r = idx % nb, c = idx / nb;
-    U[c * NB + r] = a[(j + r) + (size_t)(j + c) * lda];
+cudaError_t chol_inv_rec(double* a, int lda, double* x, int ldx, double* t, int ldt, int j0, int n, DeviceStatus* st,
+                         DescArena& arena, cudaStream_t s) {
+  if (n <= NB) {
+    chol_inv_leaf_kernel<<<1, 256, kLeafSmem, s>>>(a, lda, x, ldx, j0, n, st); note_launches();
+    return cudaGetLastError();
   }
-  const int col = c0 + blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = col < n;
-  const int T = blockDim.x, t = threadIdx.x;
-  if (active)
-    for (int r = 0; r < nb; ++r) X[r * T + t] = a[(j + r) + (size_t)col * lda];
-  __syncthreads();
-  if (!active) return;
-  for (int i = 0; i < nb; ++i) {
-    double v = X[i * T + t];
-    for (int k = 0; k < i; ++k) v -= U[i * NB + k] * X[k * T + t];
-    X[i * T + t] = v / U[i * NB + i];
-  }
-  for (int r = 0; r < nb; ++r) a[(j + r) + (size_t)col * lda] = X[r * T + t];
-}
-
-// Inverse of each upper-triangular diagonal block of size <= NB, in place in shared memory column by column
-// (X(j,j) = 1/U(j,j); X(0:j-1, j) = -X(j,j) X(0:j-1, 0:j-1) U(0:j-1, j), the leading block already inverted);
-// x is zero below the diagonal of the block on exit.
-__global__ void trtri_diag_kernel(int n, const double* u, int ldu, double* x, int ldx) {
-  __shared__ double A[NB][NB + 1];  // A[r][c]
-  __shared__ double col[NB];
-  const int j = blockIdx.x * NB;
-  const int nb = min(NB, n - j);
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int r = idx % nb, c = idx / nb;
-    A[r][c] = (r <= c) ? u[(j + r) + (size_t)(j + c) * ldu] : 0.0;
-  }
-  __syncthreads();
-  for (int c = 0; c < nb; ++c) {
-    for (int r = threadIdx.x; r < c; r += blockDim.x) col[r] = A[r][c];
-    __syncthreads();
-    const double xjj = 1.0 / A[c][c];
-    for (int r = threadIdx.x; r < c; r += blockDim.x) {
-      double acc = 0.0;
-      for (int k = r; k < c; ++k) acc += A[r][k] * col[k];
-      A[r][c] = -xjj * acc;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) A[c][c] = xjj;
-    __syncthreads();
-  }
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int r = idx % nb, c = idx / nb;
-    x[(j + r) + (size_t)(j + c) * ldx] = A[r][c];
-  }
+  const int n1 = ((n / 2 + NB - 1) / NB) * NB, n2 = n - n1;
+  cudaError_t err = chol_inv_rec(a, lda, x, ldx, t, ldt, j0, n1, st, arena, s);
+  if (err != cudaSuccess) return err;
+  double* a12 = a + j0 + (size_t)(j0 + n1) * lda;
+  double* a22 = a + (j0 + n1) + (size_t)(j0 + n1) * lda;
+  double* x11 = x + j0 + (size_t)j0 * ldx;
+  double* x12 = x + j0 + (size_t)(j0 + n1) * ldx;
+  double* x22 = x + (j0 + n1) + (size_t)(j0 + n1) * ldx;
+  double* t12 = t + j0 + (size_t)(j0 + n1) * ldt;
+  // U12 = X11^T A12 (op(A) = X11^T is lower triangular), staged in t then copied over A12.
+  GemmDesc<double> p = gemm_problem<double>(n1, n2, n1, 1.0, x11, ldx, 1, a12, lda, 0, 0.0, t12, ldt, kTriALower);
+  if ((err = gemm_group<double>(arena, &p, 1, s)) != cudaSuccess) return err;
+  copy_matrix<double>(n1, n2, t12, ldt, a12, lda, s);
+  // A22 -= U12^T U12 (upper triangle).
+  p = gemm_problem<double>(n2, n2, n1, -1.0, a12, lda, 1, a12, lda, 0, 1.0, a22, lda, kCUpper);
+  if ((err = gemm_group<double>(arena, &p, 1, s)) != cudaSuccess) return err;
+  if ((err = chol_inv_rec(a, lda, x, ldx, t, ldt, j0 + n1, n2, st, arena, s)) != cudaSuccess) return err;
+  // X12 = -X11 (U12 X22).
+  p = gemm_problem<double>(n1, n2, n2, 1.0, a12, lda, 0, x22, ldx, 0, 0.0, t12, ldt, kTriBUpper);
+  if ((err = gemm_group<double>(arena, &p, 1, s)) != cudaSuccess) return err;
+  p = gemm_problem<double>(n1, n2, n1, -1.0, x11, ldx, 0, t12, ldt, 0, 0.0, x12, ldx, kTriAUpper);
+  return gemm_group<double>(arena, &p, 1, s);
 }
 
 }  // namespace
 
-cudaError_t potrf_upper(int n, double* a, int lda, DeviceStatus* st, DescArena& arena, cudaStream_t s) {
-  const int trsm_threads = 128;
-  const size_t trsm_smem = (size_t)(NB * NB + NB * trsm_threads) * sizeof(double);
-  cudaError_t err = cudaFuncSetAttribute(potrf_trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)trsm_smem);
-  if (err != cudaSuccess) return err;
-  for (int j = 0; j < n; j += NB) {
-    const int nb = std::min(NB, n - j);
-    potrf_diag_kernel<<<1, 256, 0, s>>>(n, a, lda, j, st); note_launches();
-    const int rest = n - j - nb;
-    if (rest <= 0) break;
-    potrf_trsm_kernel<<<(rest + trsm_threads - 1) / trsm_threads, trsm_threads, trsm_smem, s>>>(n, a, lda, j, st); note_launches();
-    // A22 -= U12^T U12 (upper tiles only).
-    double* u12 = a + j + (size_t)(j + nb) * lda;
-    double* a22 = a + (j + nb) + (size_t)(j + nb) * lda;
-    GemmDesc<double> p = gemm_problem<double>(rest, rest, nb, -1.0, u12, lda, 1, u12, lda, 0, 1.0, a22, lda, kCUpper);
-    err = gemm_group<double>(arena, &p, 1, s);
-    if (err != cudaSuccess) return err;
-  }
-  return cudaGetLastError();
-}
-
-cudaError_t trtri_upper(int n, const double* u, int ldu, double* x, int ldx, double* tmp, DescArena& arena,
-                        cudaStream_t s) {
+cudaError_t potrf_inverse_upper(int n, double* a, int lda, double* x, int ldx, double* t, DeviceStatus* st,
+                                DescArena& arena, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  cudaError_t err = cudaMemsetAsync(x, 0, sizeof(double) * ((size_t)ldx * (n - 1) + n), s);
+  cudaError_t err = cudaFuncSetAttribute(chol_inv_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kLeafSmem);
   if (err != cudaSuccess) return err;
-  const int nblk = (n + NB - 1) / NB;
-  trtri_diag_kernel<<<nblk, 128, 0, s>>>(n, u, ldu, x, ldx); note_launches();
-  std::vector<GemmDesc<double>> p1, p2;
-  for (int sz = NB; sz < n; sz *= 2) {
-    p1.clear();
-    p2.clear();
-    for (int p = 0; p + sz < n; p += 2 * sz) {
-      const int s2 = std::min(sz, n - p - sz);
-      const double* u12 = u + p + (size_t)(p + sz) * ldu;
-      const double* x22 = x + (p + sz) + (size_t)(p + sz) * ldx;
-      const double* x11 = x + p + (size_t)p * ldx;
-      double* t12 = tmp + p + (size_t)(p + sz) * n;
-      double* x12 = x + p + (size_t)(p + sz) * ldx;
-      p1.push_back(gemm_problem<double>(sz, s2, s2, 1.0, u12, ldu, 0, x22, ldx, 0, 0.0, t12, n, kTriBUpper));
-      p2.push_back(gemm_problem<double>(sz, s2, sz, -1.0, x11, ldx, 0, t12, n, 0, 0.0, x12, ldx, kTriAUpper));
-    }
-    err = gemm_group<double>(arena, p1.data(), (int)p1.size(), s);
-    if (err != cudaSuccess) return err;
-    err = gemm_group<double>(arena, p2.data(), (int)p2.size(), s);
-    if (err != cudaSuccess) return err;
-  }
-  return cudaGetLastError();
+  err = cudaMemsetAsync(x, 0, sizeof(double) * ((size_t)ldx * (n - 1) + n), s);
+  if (err != cudaSuccess) return err;
+  return chol_inv_rec(a, lda, x, ldx, t, n, 0, n, st, arena, s);
 }
 
 }  // namespace xtbeig

@@ -80,6 +80,14 @@ struct DcBufs {
 
 constexpr double kEps = 1.1102230246251565e-16;
 
+// Ordering key: NaN sorts as +inf, so every ranking below is a bijection even on non-finite input (a failed earlier
+// stage must never turn into an out-of-range index).
+__device__ __forceinline__ double okey(double x) { return x == x ? x : INFINITY; }
+
+// Every level kernel returns at once when an earlier stage (or an earlier kernel of this solve) recorded an error.
+#define DC_RETURN_IF_FAILED(B) \
+  if (ld_volatile_i32(&(B).st->code) != 0) return;
+
 // ------------------------------------------------------------------------------------------------ set-up kernels
 
 __global__ void dc_scale_kernel(int n, const double* d, const double* e, double* scale) {
@@ -147,6 +155,7 @@ __global__ void __launch_bounds__(1024) dc_deflate_kernel(DcBufs B, int nmerge) 
   __shared__ int s_cnt[8];
   const int mi = blockIdx.x;
   if (mi >= nmerge) return;
+  DC_RETURN_IF_FAILED(B)
   const MergeDesc md = B.merges[mi];
   const int s = md.s, n1 = md.n1, n2 = md.n2, n = n1 + n2;
   const size_t ld = B.ld;
@@ -169,14 +178,14 @@ __global__ void __launch_bounds__(1024) dc_deflate_kernel(DcBufs B, int nmerge) 
       dv = dd[i];
       zv = B.Qa[(size_t)(s + n1 - 1) + (size_t)(s + i) * ld] * rs2;
       int lo = 0, hi = n2;  // count second-half values < dv
-      while (lo < hi) { int m = (lo + hi) >> 1; if (dd[n1 + m] < dv) lo = m + 1; else hi = m; }
+      while (lo < hi) { int m = (lo + hi) >> 1; if (okey(dd[n1 + m]) < okey(dv)) lo = m + 1; else hi = m; }
       rank = i + lo;
     } else {
       const int j = i - n1;
       dv = dd[i];
       zv = sgn * B.Qa[(size_t)(s + n1) + (size_t)(s + i) * ld] * rs2;
       int lo = 0, hi = n1;  // count first-half values <= dv
-      while (lo < hi) { int m = (lo + hi) >> 1; if (dd[m] <= dv) lo = m + 1; else hi = m; }
+      while (lo < hi) { int m = (lo + hi) >> 1; if (okey(dd[m]) <= okey(dv)) lo = m + 1; else hi = m; }
       rank = j + lo;
     }
     sd[rank] = dv;
@@ -252,7 +261,7 @@ __global__ void __launch_bounds__(1024) dc_deflate_kernel(DcBufs B, int nmerge) 
   // Survivors in position order (their values ascend), their type-grouped GEMM slots, deflated list.
   // Pass 1: counts per type.
   int cnt[4] = {0, 0, 0, 0};
-  for (int p = threadIdx.x; p < n; p += blockDim.x) cnt[typ[p] - 1]++;
+  for (int p = threadIdx.x; p < n; p += blockDim.x) cnt[min(max(typ[p], 1), 4) - 1]++;
   for (int t = 0; t < 4; ++t) {
     int tot;
     (void)block_exscan(cnt[t], s_scan, &tot);
@@ -318,11 +327,13 @@ __global__ void __launch_bounds__(1024) dc_deflate_kernel(DcBufs B, int nmerge) 
 
 // ------------------------------------------------------------------------------------------------ rotate + gather
 
-// grid (merges, row blocks); one thread per row of the merge block.
-__global__ void dc_rotate_gather_kernel(DcBufs B) {
+// grid (merges, row blocks); one thread per row applies the merge's recorded rotations in order (rows are independent).
+__global__ void dc_rotate_kernel(DcBufs B) {
+  DC_RETURN_IF_FAILED(B)
   const int mi = blockIdx.x;
-  const MergeDesc md = B.merges[mi];
   const MergeInfo inf = B.info[mi];
+  if (inf.nrot == 0) return;
+  const MergeDesc md = B.merges[mi];
   const int s = md.s, n = md.n1 + md.n2;
   const size_t ld = B.ld;
   const int r = blockIdx.y * blockDim.x + threadIdx.x;
@@ -335,8 +346,22 @@ __global__ void dc_rotate_gather_kernel(DcBufs B) {
     qrow[(size_t)i * ld] = c * qi + sn * qj;
     qrow[(size_t)j * ld] = -sn * qi + c * qj;
   }
+}
+
+// grid (merges, row blocks of blockDim.x, column chunks of 32): columns gathered into Qc in GEMM slot order.
+__global__ void dc_gather_kernel(DcBufs B) {
+  DC_RETURN_IF_FAILED(B)
+  const int mi = blockIdx.x;
+  const MergeDesc md = B.merges[mi];
+  const int s = md.s, n = md.n1 + md.n2;
+  const int r = blockIdx.y * blockDim.x + threadIdx.x;
+  const int c0 = blockIdx.z * 32;
+  if (r >= n || c0 >= n) return;
+  const size_t ld = B.ld;
+  const double* qrow = B.Qa + (size_t)(s + r) + (size_t)s * ld;
   double* crow = B.Qc + (size_t)(s + r) + (size_t)s * ld;
-  for (int col = 0; col < n; ++col) crow[(size_t)col * ld] = qrow[(size_t)B.srcCol[s + col] * ld];
+  const int c1 = min(c0 + 32, n);
+  for (int col = c0; col < c1; ++col) crow[(size_t)col * ld] = qrow[(size_t)B.srcCol[s + col] * ld];
 }
 
 // ------------------------------------------------------------------------------------------------ secular equation
@@ -444,6 +469,7 @@ __global__ void dc_secular_kernel(DcBufs B) {
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (gw >= B.n) return;
+  DC_RETURN_IF_FAILED(B)
   const int mi = B.posMerge[gw];
   if (mi < 0) return;
   const MergeDesc md = B.merges[mi];
@@ -468,6 +494,7 @@ __global__ void dc_zhat_kernel(DcBufs B) {
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (gw >= B.n) return;
+  DC_RETURN_IF_FAILED(B)
   const int mi = B.posMerge[gw];
   if (mi < 0) return;
   const MergeDesc md = B.merges[mi];
@@ -494,6 +521,7 @@ __global__ void dc_vectors_kernel(DcBufs B) {
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (gw >= B.n) return;
+  DC_RETURN_IF_FAILED(B)
   const int mi = B.posMerge[gw];
   if (mi < 0) return;
   const MergeDesc md = B.merges[mi];
@@ -521,6 +549,7 @@ __global__ void dc_vectors_kernel(DcBufs B) {
 
 // One CTA per merge: rank of every root and deflated value in the merged ascending order.
 __global__ void dc_order_kernel(DcBufs B, double* dnext) {
+  DC_RETURN_IF_FAILED(B)
   const int mi = blockIdx.x;
   const MergeDesc md = B.merges[mi];
   const MergeInfo inf = B.info[mi];
@@ -530,7 +559,7 @@ __global__ void dc_order_kernel(DcBufs B, double* dnext) {
   for (int j = threadIdx.x; j < K; j += blockDim.x) {
     const double x = lam[j];
     int c = 0;
-    for (int t = 0; t < nd; ++t) c += dv[t] < x;
+    for (int t = 0; t < nd; ++t) c += okey(dv[t]) < okey(x);
     const int rank = j + c;
     B.outSrc[s + rank] = j;
     dnext[s + rank] = x;
@@ -538,9 +567,9 @@ __global__ void dc_order_kernel(DcBufs B, double* dnext) {
   for (int t = threadIdx.x; t < nd; t += blockDim.x) {
     const double x = dv[t];
     int lo = 0, hi = K;  // roots <= x
-    while (lo < hi) { int m = (lo + hi) >> 1; if (lam[m] <= x) lo = m + 1; else hi = m; }
+    while (lo < hi) { int m = (lo + hi) >> 1; if (okey(lam[m]) <= okey(x)) lo = m + 1; else hi = m; }
     int c = lo;
-    for (int u = 0; u < nd; ++u) c += (dv[u] < x) || (dv[u] == x && u < t);
+    for (int u = 0; u < nd; ++u) c += (okey(dv[u]) < okey(x)) || (okey(dv[u]) == okey(x) && u < t);
     B.outSrc[s + c] = K + t;
     dnext[s + c] = x;
   }
@@ -548,6 +577,7 @@ __global__ void dc_order_kernel(DcBufs B, double* dnext) {
 
 // grid (merges, column blocks of 8): copy each output column into the next level's eigenvector matrix.
 __global__ void dc_copy_kernel(DcBufs B) {
+  DC_RETURN_IF_FAILED(B)
   const int mi = blockIdx.x;
   const MergeDesc md = B.merges[mi];
   const MergeInfo inf = B.info[mi];
@@ -614,11 +644,21 @@ size_t stedc_work_bytes(int n) {
   return b;
 }
 
-cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* work, size_t work_bytes,
-                         void* hstage, size_t hstage_bytes, DeviceStatus* st, cudaStream_t s) {
+size_t stedc_plan_bytes(int n) {
+  size_t b = 0;
+  auto add = [&](size_t bytes) { b += ((bytes + 255) / 256) * 256; };
+  add((size_t)32 * n * sizeof(int));
+  add((size_t)32 * (n / 2 + 2) * sizeof(MergeDesc));
+  add((size_t)32 * (n + 4) * sizeof(GemmDesc<double>));
+  return b;
+}
+
+cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* work, size_t work_bytes, void* plan,
+                         bool upload_plan, void* hstage, size_t hstage_bytes, DeviceStatus* st, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   if (work_bytes < stedc_work_bytes(n)) return cudaErrorInvalidValue;
   char* p = reinterpret_cast<char*>(work);
+  char* pp = reinterpret_cast<char*>(plan);
   DcBufs B{};
   B.n = n;
   B.ld = n;
@@ -650,10 +690,12 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
   B.outSrc = carve<int>(p, n);
   B.rotI = carve<int>(p, n);
   B.rotJ = carve<int>(p, n);
-  int* posAll = carve<int>(p, (size_t)32 * n);
-  MergeDesc* mergesAll = carve<MergeDesc>(p, (size_t)32 * (n / 2 + 2));
   B.info = carve<MergeInfo>(p, (size_t)(n / 2 + 2));
-  GemmDesc<double>* gAll = carve<GemmDesc<double>>(p, (size_t)32 * (n + 4));
+  // The plan (per-level position map, merges, merge-GEMM descriptor skeletons) depends on n only and lives in its
+  // own buffer, uploaded once per n: a captured graph never reads host staging that a later call rewrites.
+  int* posAll = carve<int>(pp, (size_t)32 * n);
+  MergeDesc* mergesAll = carve<MergeDesc>(pp, (size_t)32 * (n / 2 + 2));
+  GemmDesc<double>* gAll = carve<GemmDesc<double>>(pp, (size_t)32 * (n + 4));
   B.st = st;
 
   // Host plan: levels bottom-up (deepest first).
@@ -673,36 +715,42 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
     need = (need + 15) & ~size_t(15);
     offG[l] = need; need += 2 * levels[l].merges.size() * sizeof(GemmDesc<double>);
   }
-  if (need > hstage_bytes) return cudaErrorInvalidValue;
+  if (upload_plan && need > hstage_bytes) return cudaErrorInvalidValue;
   char* h = reinterpret_cast<char*>(hstage);
   for (int l = 0; l < L; ++l) {
-    int* pos = reinterpret_cast<int*>(h + offPos[l]);
-    for (int i = 0; i < n; ++i) pos[i] = -1;  // -1: an unmerged leaf at this level
     const auto& ms = levels[l].merges;
-    std::memcpy(h + offMer[l], ms.data(), ms.size() * sizeof(MergeDesc));
-    GemmDesc<double>* g = reinterpret_cast<GemmDesc<double>*>(h + offG[l]);
+    int* pos = upload_plan ? reinterpret_cast<int*>(h + offPos[l]) : nullptr;
+    if (pos) {
+      for (int i = 0; i < n; ++i) pos[i] = -1;  // -1: an unmerged leaf at this level
+      std::memcpy(h + offMer[l], ms.data(), ms.size() * sizeof(MergeDesc));
+    }
+    GemmDesc<double>* g = upload_plan ? reinterpret_cast<GemmDesc<double>*>(h + offG[l]) : nullptr;
     int tb = 0;
     for (size_t mi = 0; mi < ms.size(); ++mi) {
-      for (int i = 0; i < ms[mi].n1 + ms[mi].n2; ++i) pos[ms[mi].s + i] = (int)mi;
+      if (pos)
+        for (int i = 0; i < ms[mi].n1 + ms[mi].n2; ++i) pos[ms[mi].s + i] = (int)mi;
       const int nmax = ms[mi].n1 + ms[mi].n2;
       for (int half = 0; half < 2; ++half) {
-        GemmDesc<double>& gd = g[2 * mi + half];
-        std::memset(&gd, 0, sizeof(gd));
-        gd.lda = n; gd.ldb = n; gd.ldc = n;
-        gd.alpha = 1.0; gd.beta = 0.0;
-        gd.transA = 0; gd.transB = 0; gd.mode = 0;
         const int mrows = half == 0 ? ms[mi].n1 : ms[mi].n2;
-        gd.tiles_m = (mrows + kGemmBM - 1) / kGemmBM;
-        gd.tiles_n = (nmax + kGemmBN - 1) / kGemmBN;
-        gd.tile_begin = tb;
-        tb += gd.tiles_m * gd.tiles_n;
+        const int tm = (mrows + kGemmBM - 1) / kGemmBM, tn = (nmax + kGemmBN - 1) / kGemmBN;
+        if (g) {
+          GemmDesc<double>& gd = g[2 * mi + half];
+          std::memset(&gd, 0, sizeof(gd));
+          gd.lda = n; gd.ldb = n; gd.ldc = n;
+          gd.alpha = 1.0; gd.beta = 0.0;
+          gd.transA = 0; gd.transB = 0; gd.mode = 0;
+          gd.tiles_m = tm;
+          gd.tiles_n = tn;
+          gd.tile_begin = tb;
+        }
+        tb += tm * tn;
       }
     }
     tiles[l] = tb;
   }
-  // Device copies: posMerge / merges / gemm descriptors per level at fixed offsets inside the work area.
+  // Device copies of the plan: posMerge / merges / gemm descriptor skeletons per level, once per n.
   cudaError_t err;
-  for (int l = 0; l < L; ++l) {
+  for (int l = 0; upload_plan && l < L; ++l) {
     const auto& ms = levels[l].merges;
     err = cudaMemcpyAsync(posAll + (size_t)l * n, h + offPos[l], (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s);
     if (err != cudaSuccess) return err;
@@ -714,6 +762,9 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
     if (err != cudaSuccess) return err;
   }
 
+  // Index arrays start at 0: an entry that a ranking on non-finite input might leave unwritten stays in range.
+  err = cudaMemsetAsync(B.sperm, 0, (size_t)((char*)(B.rotJ + n) - (char*)B.sperm), s);
+  if (err != cudaSuccess) return err;
   dc_scale_kernel<<<1, 1024, 0, s>>>(n, d, e, B.scale); note_launches();
   dc_init_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, d, e, B.dd, B.ee, B.scale); note_launches();
   {
@@ -729,7 +780,8 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
     B.gdesc = gAll + (size_t)l * (n + 4);
     const int dthreads = maxn > 512 ? 1024 : (maxn > 128 ? 512 : 128);
     dc_deflate_kernel<<<nm, dthreads, 0, s>>>(B, nm); note_launches();
-    dc_rotate_gather_kernel<<<dim3(nm, (maxn + 127) / 128), 128, 0, s>>>(B); note_launches();
+    dc_rotate_kernel<<<dim3(nm, (maxn + 127) / 128), 128, 0, s>>>(B); note_launches();
+    dc_gather_kernel<<<dim3(nm, (maxn + 127) / 128, (maxn + 31) / 32), 128, 0, s>>>(B); note_launches();
     const int warps_per_block = 8;
     const int nblk = (n + warps_per_block - 1) / warps_per_block;
     dc_secular_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();

@@ -12,12 +12,16 @@
 //      computes ||x|| with a block reduction and forms beta, tau, v exactly as every other CTA does (same data,
 //      same reduction order => bit-identical v in all CTAs, no exchange needed);
 //   2. in ONE pass over its own rows applies the previous step's rank-2 update A -= v w^T + w v^T and accumulates
-//      y_r = sum_c A(r,c) v(c) (the update of step k+1 fused with the symv of step k), writing y_r and A(r,k-1) to
-//      a double-buffered exchange vector;
-//   3. one grid barrier; then reads y (all rows) and column k-1, forms w = tau y - tau^2/2 (y.v) v and the next
-//      x = A(0:k-2, k-1) - v w(k-1) - w v(k-1) redundantly.
-// One barrier per column.  All reductions run in a fixed order, so results are deterministic and identical across
-// CTAs; the barrier waits are time-limited (status word, no trap).
+//      y_r = sum_c A(r,c) v(c) (the update of step k+1 fused with the symv of step k); the per-row partial sums are
+//      combined by a reduce-scatter across the warp's lanes (9 shuffles for 8 rows instead of 40);
+//   3. publishes (y_r, A(r,k-1)) for its rows, meets every CTA at one grid barrier (a release-add on a counter and an
+//      acquire poll, no further fences) and reads every row's pair for its columns.  Two exchange buffers alternate:
+//      a CTA writes buffer p again only two steps later, after the barrier of the step in between, which every CTA
+//      reaches only after it has read buffer p.  (Polling per-value readiness flags instead of one counter was
+//      measured slower: 75k threads polling L2 cost more than one counter round trip.);
+//   4. forms w = tau y - tau^2/2 (y.v) v and the next x = A(0:k-2, k-1) - v w(k-1) - w v(k-1) redundantly.
+// One grid barrier and three block-level syncs per column; every reduction runs in a fixed order, so results are
+// deterministic and identical across CTAs; every wait is time-limited (device status word, no trap).
 #include "common.cuh"
 #include "kernels.h"
 
@@ -25,29 +29,85 @@ namespace xtbeig {
 
 namespace {
 
-constexpr int kRowChunk = 8;  // rows whose partial dot products are reduced together
+constexpr int kRowChunk = 8;  // rows whose partial dot products are reduce-scattered together
 
+// Relaxed (morally strong) pair accesses of the exchange buffer (read after the grid barrier).
+__device__ __forceinline__ void st_pair(double* p, double a, double b) {
+  asm volatile("st.relaxed.gpu.global.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(a), "d"(b) : "memory");
+}
+__device__ __forceinline__ void ld_pair(const double* p, double& a, double& b) {
+  asm volatile("ld.relaxed.gpu.global.v2.f64 {%0, %1}, [%2];" : "=d"(a), "=d"(b) : "l"(p) : "memory");
+}
+__device__ __forceinline__ void st_pair(float* p, float a, float b) {
+  asm volatile("st.relaxed.gpu.global.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
+}
+__device__ __forceinline__ void ld_pair(const float* p, float& a, float& b) {
+  asm volatile("ld.relaxed.gpu.global.v2.f32 {%0, %1}, [%2];" : "=f"(a), "=f"(b) : "l"(p) : "memory");
+}
+
+// Block sum with a compile-time warp count: one __syncthreads; `scratch` (NW values) must not be reused by another
+// block_sum before every thread has passed this call's __syncthreads and read it (callers rotate scratch slots).
+template <int NW, typename T>
+__device__ __forceinline__ T block_sum_nw(T v, T* scratch) {
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) scratch[threadIdx.x >> 5] = v;
+  __syncthreads();
+  T r = T(0);
+#pragma unroll
+  for (int w = 0; w < NW; ++w) r += scratch[w];
+  return r;
+}
+
+// Reduce-scatter of 8 per-lane partial sums across the warp: on return lane l holds the warp-wide sum of row
+// (l >> 2) & 7 (complete in lanes with (l & 3) == 0).
 template <typename T>
-__device__ __forceinline__ T ld_cg(const T* p) { return __ldcg(p); }
+__device__ __forceinline__ T warp_reduce_scatter8(T (&acc)[kRowChunk]) {
+  const unsigned lane = threadIdx.x & 31;
+  const bool h4 = lane & 16, h3 = lane & 8, h2 = lane & 4;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const T send = h4 ? acc[i] : acc[i + 4];
+    const T keep = h4 ? acc[i + 4] : acc[i];
+    acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const T send = h3 ? acc[i] : acc[i + 2];
+    const T keep = h3 ? acc[i + 2] : acc[i];
+    acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  {
+    const T send = h2 ? acc[0] : acc[1];
+    const T keep = h2 ? acc[1] : acc[0];
+    acc[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  T r = acc[0];
+  r += __shfl_xor_sync(0xffffffffu, r, 2);
+  r += __shfl_xor_sync(0xffffffffu, r, 1);
+  return r;
+}
 
 // kUpperInPlace: the variant that reads the upper triangle of p.afull (== p.aout) in place instead of a full
-// symmetric copy, and therefore waits at one extra grid barrier after loading, before any CTA writes the matrix.
-template <typename T, int NT, int CPT, bool kUpperInPlace = false>
+// symmetric copy, and therefore waits at one grid barrier after loading, before any CTA writes the matrix.
+// kSmemRows: rows resident in shared memory (known at compile time, so row accesses are shared-memory instructions).
+template <typename T, int NT, int CPT, bool kUpperInPlace = false, bool kSmemRows = true>
 __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p) {
   constexpr int NW = NT / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int n = p.n, R = p.rows_per_cta;
   const size_t ldr = (size_t)p.ldr;
+  if (ld_volatile_i32(&p.st->code) != 0) return;  // an earlier stage failed: every CTA skips the reduction
 
   T* red = reinterpret_cast<T*>(smem_raw);  // [R][NW] per-warp partial row sums
   T* vrow = red + (size_t)R * NW;           // [R] previous v at own rows
   T* wrow = vrow + R;                       // [R] previous w at own rows
-  T* bred = wrow + R;                       // [NW] block-reduction scratch
-  T* scal = bred + NW;                      // [8] broadcast scalars
+  T* colk = wrow + R;                       // [R] A(r, k-1) captured by the pass
+  T* bred = colk + R;                       // [3][NW] block-reduction scratch (rotated)
+  T* scal = bred + 3 * NW;                  // [8] broadcast scalars
   T* rows;
-  if (p.use_smem) {
-    size_t off = (size_t)(R * NW + 2 * R + NW + 8) * sizeof(T);
+  if constexpr (kSmemRows) {
+    size_t off = (size_t)(R * NW + 3 * R + 3 * NW + 8) * sizeof(T);
     off = (off + 15) & ~size_t(15);
     rows = reinterpret_cast<T*>(smem_raw + off);
   } else {
@@ -82,11 +142,12 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
   __syncthreads();
 
   unsigned epoch = 0;
-  int par = 0;
   if constexpr (kUpperInPlace) {
     if (!group_barrier(p.counter, (unsigned)G, epoch, p.st, p.limit_ns)) return;
   }
   for (int k = n - 1; k >= 1; --k) {
+    const int t = n - 1 - k;                   // step index
+    T* xch = p.xch + (size_t)(t & 1) * 2 * n;  // (y, column) pairs of this step
     const bool has_prev = (k < n - 1);
     // ---- 1. Householder vector from x = A(0:k-1, k); alpha = x(k-1).
     const int tk = (k - 1) % NT, jk = (k - 1) / NT;
@@ -97,7 +158,7 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
       if (c < k - 1) part += x[j] * x[j];
       if (tid == tk && j == jk) scal[0] = x[j];
     }
-    const T xn2 = block_sum(part, bred);  // contains __syncthreads: scal[0] visible
+    const T xn2 = block_sum_nw<NW>(part, bred);  // its __syncthreads also publishes scal[0], vrow, wrow
     const T alpha = scal[0];
     T beta, tau, scale;
     if (xn2 == T(0)) {
@@ -125,8 +186,6 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
     }
 
     // ---- 2. fused pass: previous rank-2 update + y = A v over own rows r < k.
-    T* ybuf = p.ybuf + (size_t)par * n;
-    T* cbuf = p.cbuf + (size_t)par * n;
     for (int q0 = 0; q0 < R; q0 += kRowChunk) {
       if (cta + q0 * G >= k) break;
       T acc[kRowChunk];
@@ -148,80 +207,73 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
                 row[c] = a;
               }
               acc[qq] += a * vn[j];
-              if (c == k - 1) cbuf[r] = a;
+              if (c == k - 1) colk[q] = a;
             }
           }
         }
       }
-#pragma unroll
-      for (int qq = 0; qq < kRowChunk; ++qq) acc[qq] = warp_sum(acc[qq]);
-      if (lane == 0) {
-#pragma unroll
-        for (int qq = 0; qq < kRowChunk; ++qq)
-          if (q0 + qq < R) red[(q0 + qq) * NW + warp] = acc[qq];
-      }
+      const T rs = warp_reduce_scatter8(acc);
+      const int qrow = q0 + ((lane >> 2) & 7);
+      if ((lane & 3) == 0 && qrow < R) red[qrow * NW + warp] = rs;
     }
     __syncthreads();
+    // ---- 3. publish (y_r, A(r,k-1)) for own rows, then read every row's pair for this thread's columns.
     for (int q = tid; q < R; q += NT) {
       const int r = cta + q * G;
       if (r < k) {
         T y = T(0);
+#pragma unroll
         for (int w = 0; w < NW; ++w) y += red[q * NW + w];
-        ybuf[r] = y;
+        st_pair(xch + 2 * (size_t)r, y, colk[q]);
       }
     }
-
-    // ---- 3. one grid barrier, then w and the next column, redundantly in every CTA.
     if (!group_barrier(p.counter, (unsigned)G, epoch, p.st, p.limit_ns)) return;
-
     T yj[CPT], colj[CPT];
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) {
+      yj[j] = colj[j] = T(0);
+      if (tid + j * NT < k) ld_pair(xch + 2 * (size_t)(tid + j * NT), yj[j], colj[j]);
+    }
+    // y(k-1) and A(k-1,k-1) for w(k-1) and d(k-1), published through the same __syncthreads as y.v.
     T pyv = T(0);
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
-      const int c = tid + j * NT;
-      yj[j] = c < k ? ld_cg(ybuf + c) : T(0);
-      colj[j] = c < k ? ld_cg(cbuf + c) : T(0);
       pyv += yj[j] * vn[j];
+      if (tid == tk && j == jk) { scal[1] = yj[j]; scal[2] = colj[j]; }
     }
-    const T yv = block_sum(pyv, bred);
+    const T yv = block_sum_nw<NW>(pyv, bred + NW);
     const T half = T(0.5) * tau * tau * yv;
-    T w[CPT];
-#pragma unroll
-    for (int j = 0; j < CPT; ++j) {
-      w[j] = tau * yj[j] - half * vn[j];
-      if (tid == tk && j == jk) { scal[1] = w[j]; scal[2] = colj[j]; }
-    }
-    __syncthreads();
-    const T wkm1 = scal[1];
+    const T wkm1 = tau * scal[1] - half;  // v(k-1) = 1
     if (cta == 0 && tid == 0) {
-      const T dk = scal[2] - T(2) * wkm1;  // A(k-1,k-1) after this step's update (v(k-1) = 1)
+      const T dk = scal[2] - T(2) * wkm1;  // A(k-1,k-1) after this step's update
       p.d[k - 1] = dk;
       p.aout[(size_t)(k - 1) + (size_t)(k - 1) * p.lda] = dk;
     }
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
       const int c = tid + j * NT;
-      x[j] = c < k - 1 ? colj[j] - vn[j] * wkm1 - w[j] : T(0);
+      const T w = tau * yj[j] - half * vn[j];
+      x[j] = c < k - 1 ? colj[j] - vn[j] * wkm1 - w : T(0);
       vk[j] = vn[j];
-      wk[j] = w[j];
+      wk[j] = w;
       if (c < k && (c % G) == cta) {
         const int q = c / G;
         vrow[q] = vn[j];
-        wrow[q] = w[j];
+        wrow[q] = w;
       }
     }
-    __syncthreads();
-    par ^= 1;
   }
 }
 
 template <typename T, int NT, int CPT>
 cudaError_t launch_one(const SytrdParams<T>& p, int G, size_t smem, cudaStream_t s) {
-  auto kern = sytrd_resident_kernel<T, NT, CPT>;
+  auto kern = p.use_smem ? sytrd_resident_kernel<T, NT, CPT, false, true> : sytrd_resident_kernel<T, NT, CPT, false, false>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   void* args[] = {(void*)&p};
-  return cudaLaunchCooperativeKernel((void*)kern, dim3(G), dim3(NT), args, smem, s);
+  err = cudaLaunchCooperativeKernel((void*)kern, dim3(G), dim3(NT), args, smem, s);
+  note_launches();
+  return err;
 }
 
 template <int CPT>
@@ -230,7 +282,9 @@ cudaError_t launch_upper_inplace(const SytrdParams<double>& p, int G, size_t sme
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   void* args[] = {(void*)&p};
-  return cudaLaunchCooperativeKernel((void*)kern, dim3(G), dim3(512), args, smem, s);
+  err = cudaLaunchCooperativeKernel((void*)kern, dim3(G), dim3(512), args, smem, s);
+  note_launches();
+  return err;
 }
 
 }  // namespace
@@ -252,7 +306,7 @@ size_t sytrd_smem_bytes(int n, int G, int NT, bool rows_in_smem, int* R_out, int
   const int align = 16 / (int)sizeof(T);
   const int ldr = ((n + align - 1) / align) * align;
   const int NW = NT / 32;
-  size_t bytes = (size_t)(R * NW + 2 * R + NW + 8) * sizeof(T);
+  size_t bytes = (size_t)(R * NW + 3 * R + 3 * NW + 8) * sizeof(T);
   bytes = (bytes + 15) & ~size_t(15);
   if (rows_in_smem) bytes += (size_t)R * ldr * sizeof(T);
   if (R_out) *R_out = R;
@@ -264,7 +318,7 @@ template <typename T>
 SytrdPlan sytrd_plan(int n, int num_sms, size_t max_smem, int grid_override) {
   SytrdPlan pl{};
   int G = grid_override > 0 ? grid_override : num_sms;
-  // Small problems: fewer CTAs (a barrier over fewer members), at least ~4 rows each.
+  // Small problems: fewer CTAs, at least ~4 rows each.
   if (grid_override <= 0) G = max(1, min(G, (n + 3) / 4));
   pl.grid = G;
   pl.threads = 512;
