@@ -300,7 +300,10 @@ void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
   double* e = k.template dev<double>("gv.e", (size_t)n);
   double* tau = k.template dev<double>("gv.tau", (size_t)n);
   if (!k.ok()) return;
-  k.check(potrf_inverse_upper(n, u, n, x, n, t, k.c->d_status, k.c->arena, k.s), "potrf+inverse");
+  unsigned* pctr = k.template dev<unsigned>("potrf.ctr", 64);
+  if (k.ok())
+    k.check(potrf_inverse_upper(n, u, n, x, n, t, pctr, k.c->num_sms, k.c->d_status, wait_limit_ns(), k.s),
+            "potrf+inverse");
   k.mark("potrf_inverse");
   // G = H X (X upper), then H' = X^T G on the upper tiles, symmetrised for the reduction.
   GemmDesc<double> p = gemm_problem<double>(n, n, n, 1.0, h, n, 0, x, n, 0, 0.0, t, n, kTriBUpper);

@@ -121,8 +121,9 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
 // ---------------------------------------------------------------------------------------------------- potrf / trtri
 // S = U^T U (upper, in place) and X = U^-1 (upper, strict lower part zero) in one recursion; t: n x n scratch (ld n).
 // A non-SPD S records kStatusNotSPD with info = the failing column (1-based).
-cudaError_t potrf_inverse_upper(int n, double* a, int lda, double* x, int ldx, double* t, DeviceStatus* st,
-                                DescArena& arena, cudaStream_t s);
+// One persistent cooperative kernel of at most `grid` CTAs; counter: 64 unsigned barrier words.
+cudaError_t potrf_inverse_upper(int n, double* a, int lda, double* x, int ldx, double* t, unsigned* counter,
+                                int grid, DeviceStatus* st, uint64_t limit_ns, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- adjoint
 // Daleckii-Krein gradient of sum(Wbar o C diag(f) C^T): dh, ds (n x n, ld n); t1..t3 n x n scratch.

@@ -2,16 +2,22 @@
 //
 // xTB factors S once per geometry (mctc_potrf) and reduces every cycle with dsygst or with the congruence
 // H' = X^T H X, X = U^-1 (xtb #1466; reference scripts/kernels/congruence.c:1-52 studies it; EigenBench's dump reader
-// does dpotrf, dtrtri and two dtrmm: Sources/EigenBench/main.swift:167-172).  Here both factors come out of one
-// recursion:
-//     [A11 A12; . A22]:  (U11, X11) = chol_inv(A11);  U12 = X11^T A12;  A22 -= U12^T U12;
-//                        (U22, X22) = chol_inv(A22);  X12 = -X11 U12 X22,
-// every off-diagonal step a triangular-masked FP64 tensor-core GEMM, the 64 x 64 leaves factored and inverted in
-// shared memory by one CTA (two block syncs per factorization step, one per inverse column).
-// A pivot that is not > 0 (or NaN) records kStatusNotSPD with the global column (1-based), LAPACK's info; the kernels
-// of the remaining recursion then return at once.
+// does dpotrf, dtrtri and two dtrmm: Sources/EigenBench/main.swift:167-172).
+//
+// B200 design: ONE persistent cooperative kernel produces both factors (a chain of ~160 small kernels spent most of
+// its time in launch and pipeline-fill latency).  Blocks of 64 columns, right-looking, with grid barriers:
+//   step j:  B  all CTAs: block row U(j, j+1:) = X(j,j)^T A(j, j+1:)       (64 x 64 DMMA tiles, in place)
+//            --- barrier ---
+//            C  CTA 0: tile (j+1, j+1) of the trailing update, then factors and inverts that diagonal block in shared
+//               memory (look-ahead: the next step's diagonal work overlaps the rest of the update);
+//               other CTAs: the remaining upper tiles of A(j+1:, j+1:) -= U(j, j+1:)^T U(j, j+1:)
+//            --- barrier ---
+// then X by doubling over block sizes 64, 128, ...: X12 = -X11 (U12 X22), every tile of a level in parallel.
+// A pivot that is not > 0 (or NaN) records kStatusNotSPD with the global column (1-based), LAPACK's info, and every
+// CTA leaves at the next barrier.  Every barrier wait is time-limited.
 #include <algorithm>
 
+#include "gemm_tile.cuh"
 #include "kernels.h"
 
 namespace xtbeig {
@@ -19,23 +25,33 @@ namespace xtbeig {
 namespace {
 
 constexpr int NB = 64;
-constexpr size_t kLeafSmem = (size_t)(2 * NB * (NB + 1) + NB) * sizeof(double);
+constexpr int kThreads = kGemmThreads;  // 128: the tile routine's CTA shape
 
-// One CTA of 256 threads: U (upper Cholesky factor of the nb x nb block at (j0, j0), nb <= 64) in place in `a`,
-// X = U^-1 (upper, zero below the diagonal) into `x`.
-//   factor: per step k every thread forms 1/sqrt(U(k,k)) itself, the row is scaled, and the trailing triangle is
-//           updated by a 16 x 16 thread tile (two block syncs per step);
-//   invert: column by column, X(0:c-1, c) = -X(c,c) X(0:c-1, 0:c-1) U(0:c-1, c), eight threads per row each summing
-//           every eighth term, combined by three shuffles (one block sync per column).
-__global__ void __launch_bounds__(256) chol_inv_leaf_kernel(double* a, int lda, double* x, int ldx, int j0, int nb,
-                                                            DeviceStatus* st) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double(*U)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(smem_raw);
+struct PotrfParams {
+  double* a;
+  int lda;
+  double* x;
+  int ldx;
+  double* t;  // n x n scratch, ld n
+  int n;
+  unsigned* counter;
+  DeviceStatus* st;
+  uint64_t limit_ns;
+};
+
+constexpr size_t kLeafElems = (size_t)2 * NB * (NB + 1) + NB;
+constexpr size_t kSmemBytes = (tile::smem_elems<double>() + kLeafElems) * sizeof(double);
+
+// Factor and invert the nb x nb (nb <= 64) diagonal block at (j0, j0) with the CTA's 128 threads: U in place in a,
+// X = U^-1 (upper, zero below the diagonal) into x.  Returns false (all threads) on a non-positive pivot.
+__device__ bool leaf_factor_invert(double* a, int lda, double* x, int ldx, int j0, int nb, DeviceStatus* st,
+                                   double* smem) {
+  double(*U)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(smem);
   double(*X)[NB + 1] = U + NB;
   double* dinv = reinterpret_cast<double*>(X + NB);
-  if (ld_volatile_i32(&st->code) != 0) return;
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  for (int idx = tid; idx < NB * NB; idx += 256) {  // the whole 64 x 64 frame: zero outside the nb x nb block
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;  // 16 x 8 thread tile
+  __syncthreads();  // the block may just have been written by this CTA's other threads (the look-ahead tile update)
+  for (int idx = tid; idx < NB * NB; idx += kThreads) {  // the whole 64 x 64 frame: zero outside the block
     const int r = idx % NB, c = idx / NB;
     U[r][c] = (r <= c && c < nb) ? a[(j0 + r) + (size_t)(j0 + c) * lda] : 0.0;
     X[r][c] = 0.0;
@@ -45,18 +61,20 @@ __global__ void __launch_bounds__(256) chol_inv_leaf_kernel(double* a, int lda, 
     const double piv = U[k][k];
     if (!(piv > 0.0)) {
       if (tid == 0) set_status(st, kStatusNotSPD, j0 + k + 1, 0);
-      return;  // uniform: every thread read the same pivot
+      __syncthreads();
+      return false;  // uniform: every thread read the same pivot
     }
     const double inv = rsqrt(piv), u = piv * inv;  // one reciprocal square root on the step's critical path
     const int c = k + 1 + tid;
     if (c < nb) U[k][c] *= inv;
     __syncthreads();
-    for (int i = 0; i < 4; ++i) {
-      const int r = k + 1 + ty + 16 * i;
+    for (int i = 0; i < 8; ++i) {
+      const int r = k + 1 + ty + 8 * i;
       if (r >= nb) break;
       const double ukr = U[k][r];
-      for (int j = 0; j < 4; ++j) {
-        const int cc = k + 1 + tx + 16 * j;
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const int cc = k + 1 + tx + 16 * jj;
         if (cc >= r && cc < nb) U[r][cc] -= ukr * U[k][cc];
       }
     }
@@ -66,14 +84,13 @@ __global__ void __launch_bounds__(256) chol_inv_leaf_kernel(double* a, int lda, 
     }
     __syncthreads();
   }
-  for (int idx = tid; idx < nb * nb; idx += 256) {
+  for (int idx = tid; idx < nb * nb; idx += kThreads) {
     const int r = idx % nb, c = idx / nb;
     if (r <= c) a[(j0 + r) + (size_t)(j0 + c) * lda] = U[r][c];
   }
-  // Inverse by doubling: the 8 x 8 diagonal blocks by back substitution (one thread per column), then for block
-  // sizes s = 8, 16, 32 every pair of neighbouring inverted blocks is joined: T = U12 X22, X12 = -X11 T.  The
-  // sub-diagonal part of U is zero and padding rows/columns beyond nb act as identity-free zeros, so the joins can
-  // run over the full 64 x 64 frame; only entries < nb are written back.
+  // Inverse by doubling inside the block: 8 x 8 diagonal blocks by back substitution (one thread per column), then
+  // joins of neighbouring blocks for sizes 8, 16, 32: T = U12 X22 (kept transposed in U's unused strict lower part),
+  // X12 = -X11 T.  The frame beyond nb is zero, so the joins can run over the full 64 x 64 frame.
   if (tid < NB) {
     const int c = tid, b0 = (c / 8) * 8;
     if (c < nb) {
@@ -87,19 +104,16 @@ __global__ void __launch_bounds__(256) chol_inv_leaf_kernel(double* a, int lda, 
   }
   __syncthreads();
   for (int sz = 8; sz < NB; sz *= 2) {
-    // T = U12 X22 for every pair (block rows p..p+sz, block cols p+sz..p+2sz), stored in the strict lower part of U
-    // transposed: T(r, c) -> U[c][r] (c > r always, so this area is unused).
     const int npair = NB / (2 * sz);
-    for (int idx = tid; idx < npair * sz * sz; idx += 256) {
+    for (int idx = tid; idx < npair * sz * sz; idx += kThreads) {
       const int pr = idx / (sz * sz), rem = idx % (sz * sz);
       const int r = pr * 2 * sz + rem % sz, c = pr * 2 * sz + sz + rem / sz;
       double sacc = 0.0;
-      const int q0 = pr * 2 * sz + sz;
-      for (int q = q0; q <= c; ++q) sacc += U[r][q] * X[q][c];
+      for (int q = pr * 2 * sz + sz; q <= c; ++q) sacc += U[r][q] * X[q][c];
       U[c][r] = sacc;
     }
     __syncthreads();
-    for (int idx = tid; idx < npair * sz * sz; idx += 256) {
+    for (int idx = tid; idx < npair * sz * sz; idx += kThreads) {
       const int pr = idx / (sz * sz), rem = idx % (sz * sz);
       const int r = pr * 2 * sz + rem % sz, c = pr * 2 * sz + sz + rem / sz;
       double sacc = 0.0;
@@ -109,53 +123,147 @@ __global__ void __launch_bounds__(256) chol_inv_leaf_kernel(double* a, int lda, 
     }
     __syncthreads();
   }
-  for (int idx = tid; idx < nb * nb; idx += 256) {
+  for (int idx = tid; idx < nb * nb; idx += kThreads) {
     const int r = idx % nb, c = idx / nb;
     x[(j0 + r) + (size_t)(j0 + c) * ldx] = X[r][c];
   }
+  __syncthreads();
+  return true;
 }
 
-cudaError_t chol_inv_rec(double* a, int lda, double* x, int ldx, double* t, int ldt, int j0, int n, DeviceStatus* st,
-                         DescArena& arena, cudaStream_t s) {
-  if (n <= NB) {
-    chol_inv_leaf_kernel<<<1, 256, kLeafSmem, s>>>(a, lda, x, ldx, j0, n, st); note_launches();
-    return cudaGetLastError();
+__device__ __forceinline__ GemmDesc<double> tile_desc(int M, int N, int K, double alpha, const double* A, int lda,
+                                                      int transA, const double* B, int ldb, double beta, double* C,
+                                                      int ldc, int mode) {
+  GemmDesc<double> d{};
+  d.A = A; d.B = B; d.C = C;
+  d.M = M; d.N = N; d.K = K;
+  d.lda = lda; d.ldb = ldb; d.ldc = ldc;
+  d.alpha = alpha; d.beta = beta;
+  d.transA = transA; d.transB = 0;
+  d.mode = mode;
+  return d;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) potrf_persistent_kernel(PotrfParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* gsm = reinterpret_cast<double*>(smem_raw);         // tile pipeline
+  double* lsm = gsm + tile::smem_elems<double>();            // leaf block
+  const int G = gridDim.x, cta = blockIdx.x, n = p.n;
+  const int nt = (n + NB - 1) / NB;
+  double* a = p.a;
+  double* x = p.x;
+  const int lda = p.lda, ldx = p.ldx;
+  unsigned epoch = 0;
+  if (ld_volatile_i32(&p.st->code) != 0) return;
+  auto bsize = [&](int b) { return min(NB, n - b * NB); };
+
+  if (cta == 0) leaf_factor_invert(a, lda, x, ldx, 0, bsize(0), p.st, lsm);
+  if (!group_barrier(p.counter, (unsigned)G, epoch, p.st, p.limit_ns)) return;
+  if (ld_volatile_i32(&p.st->code) != 0) return;
+
+  for (int j = 0; j + 1 < nt; ++j) {
+    const int j0 = j * NB, nbj = bsize(j);
+    // B: block row U(j, c) = X(j,j)^T A(j, c), in place (each tile reads only its own block of A).
+    for (int c = j + 1 + cta; c < nt; c += G) {
+      const int c0 = c * NB;
+      GemmDesc<double> d = tile_desc(nbj, bsize(c), nbj, 1.0, x + j0 + (size_t)j0 * ldx, ldx, 1,
+                                     a + j0 + (size_t)c0 * lda, lda, 0.0, a + j0 + (size_t)c0 * lda, lda, kTriALower);
+      tile::gemm_tile<double>(d, 0, 0, gsm);
+    }
+    if (!group_barrier(p.counter, (unsigned)G, epoch, p.st, p.limit_ns)) return;
+    // C: trailing update of the upper tiles (r, c), j < r <= c; CTA 0 takes (j+1, j+1) and then the next diagonal.
+    const int m = nt - j - 1;
+    if (cta == 0) {
+      const int r0 = (j + 1) * NB;
+      GemmDesc<double> d = tile_desc(bsize(j + 1), bsize(j + 1), nbj, -1.0, a + j0 + (size_t)r0 * lda, lda, 1,
+                                     a + j0 + (size_t)r0 * lda, lda, 1.0, a + r0 + (size_t)r0 * lda, lda, kCUpper);
+      tile::gemm_tile<double>(d, 0, 0, gsm);
+      leaf_factor_invert(a, lda, x, ldx, r0, bsize(j + 1), p.st, lsm);
+    }
+    const int ntile = m * (m + 1) / 2 - 1;  // upper tiles of the m x m trailing block, except (j+1, j+1)
+    const int workers = G > 1 ? G - 1 : 1;
+    const int me = G > 1 ? cta - 1 : 0;
+    if (G == 1 || cta > 0) {
+      for (int t = me; t < ntile; t += workers) {
+        // t -> (rr, cc) over the upper triangle by columns, skipping (0, 0): column cc holds rows 0..cc.
+        int q = t + 1, cc = 0;
+        while (q > cc) { q -= cc + 1; ++cc; }
+        const int rr = q;
+        const int r = j + 1 + rr, c = j + 1 + cc;
+        const int r0 = r * NB, c0 = c * NB;
+        GemmDesc<double> d = tile_desc(bsize(r), bsize(c), nbj, -1.0, a + j0 + (size_t)r0 * lda, lda, 1,
+                                       a + j0 + (size_t)c0 * lda, lda, 1.0, a + r0 + (size_t)c0 * lda, lda,
+                                       r == c ? kCUpper : 0);
+        tile::gemm_tile<double>(d, 0, 0, gsm);
+      }
+    }
+    if (!group_barrier(p.counter, (unsigned)G, epoch, p.st, p.limit_ns)) return;
+    if (ld_volatile_i32(&p.st->code) != 0) return;
   }
-  const int n1 = ((n / 2 + NB - 1) / NB) * NB, n2 = n - n1;
-  cudaError_t err = chol_inv_rec(a, lda, x, ldx, t, ldt, j0, n1, st, arena, s);
-  if (err != cudaSuccess) return err;
-  double* a12 = a + j0 + (size_t)(j0 + n1) * lda;
-  double* a22 = a + (j0 + n1) + (size_t)(j0 + n1) * lda;
-  double* x11 = x + j0 + (size_t)j0 * ldx;
-  double* x12 = x + j0 + (size_t)(j0 + n1) * ldx;
-  double* x22 = x + (j0 + n1) + (size_t)(j0 + n1) * ldx;
-  double* t12 = t + j0 + (size_t)(j0 + n1) * ldt;
-  // U12 = X11^T A12 (op(A) = X11^T is lower triangular), staged in t then copied over A12.
-  GemmDesc<double> p = gemm_problem<double>(n1, n2, n1, 1.0, x11, ldx, 1, a12, lda, 0, 0.0, t12, ldt, kTriALower);
-  if ((err = gemm_group<double>(arena, &p, 1, s)) != cudaSuccess) return err;
-  copy_matrix<double>(n1, n2, t12, ldt, a12, lda, s);
-  // A22 -= U12^T U12 (upper triangle).
-  p = gemm_problem<double>(n2, n2, n1, -1.0, a12, lda, 1, a12, lda, 0, 1.0, a22, lda, kCUpper);
-  if ((err = gemm_group<double>(arena, &p, 1, s)) != cudaSuccess) return err;
-  if ((err = chol_inv_rec(a, lda, x, ldx, t, ldt, j0 + n1, n2, st, arena, s)) != cudaSuccess) return err;
-  // X12 = -X11 (U12 X22).
-  p = gemm_problem<double>(n1, n2, n2, 1.0, a12, lda, 0, x22, ldx, 0, 0.0, t12, ldt, kTriBUpper);
-  if ((err = gemm_group<double>(arena, &p, 1, s)) != cudaSuccess) return err;
-  p = gemm_problem<double>(n1, n2, n1, -1.0, x11, ldx, 0, t12, ldt, 0, 0.0, x12, ldx, kTriAUpper);
-  return gemm_group<double>(arena, &p, 1, s);
+
+  // X by doubling over block pairs: T = U12 X22 (scratch t), X12 = -X11 T.
+  for (int sz = NB; sz < n; sz *= 2) {
+    const int tb = sz / NB;  // blocks per half
+    const int pairs = (n + 2 * sz - 1) / (2 * sz);
+    // tiles of all pairs: (pair, row block in first half, column block in second half)
+    int total = 0;
+    for (int pr = 0; pr < pairs; ++pr) {
+      const int p0 = pr * 2 * sz, s2 = min(sz, n - p0 - sz);
+      if (s2 > 0) total += tb * ((s2 + NB - 1) / NB);
+    }
+    for (int phase = 0; phase < 2; ++phase) {
+      for (int t = cta; t < total; t += G) {
+        int rem = t, pr = 0;
+        for (;; ++pr) {
+          const int p0 = pr * 2 * sz, s2 = min(sz, n - p0 - sz);
+          const int cnt = s2 > 0 ? tb * ((s2 + NB - 1) / NB) : 0;
+          if (rem < cnt) break;
+          rem -= cnt;
+        }
+        const int p0 = pr * 2 * sz, s2 = min(sz, n - p0 - sz);
+        const int rb = rem % tb, cb = rem / tb;
+        const int r0 = p0 + rb * NB, c0 = p0 + sz + cb * NB;
+        const int rows = NB, cols = min(NB, p0 + sz + s2 - c0);
+        double* tt = p.t + r0 + (size_t)c0 * n;
+        if (phase == 0) {
+          // T(r0 block, c0 block) = U(r0, p0+sz : p0+sz+s2) X(p0+sz : , c0): K over the second half (X22 upper).
+          GemmDesc<double> d = tile_desc(rows, cols, s2, 1.0, a + r0 + (size_t)(p0 + sz) * lda, lda, 0,
+                                         x + (p0 + sz) + (size_t)c0 * ldx, ldx, 0.0, tt, n, 0);
+          d.mode = 0;
+          // X22 is upper triangular: rows of the second half beyond the column block are zero.
+          d.K = min(s2, c0 + cols - (p0 + sz));
+          tile::gemm_tile<double>(d, 0, 0, gsm);
+        } else {
+          // X(r0 block, c0 block) = -X(r0, p0 : p0+sz) T(p0 : p0+sz, c0): X11 upper, so K starts at the row block.
+          const int k0 = r0 - p0;
+          GemmDesc<double> d = tile_desc(rows, cols, sz - k0, -1.0, x + r0 + (size_t)r0 * ldx, ldx, 0,
+                                         p.t + r0 + (size_t)c0 * n, n, 0.0, x + r0 + (size_t)c0 * ldx, ldx, 0);
+          tile::gemm_tile<double>(d, 0, 0, gsm);
+        }
+      }
+      if (!group_barrier(p.counter, (unsigned)G, epoch, p.st, p.limit_ns)) return;
+    }
+  }
 }
 
 }  // namespace
 
-cudaError_t potrf_inverse_upper(int n, double* a, int lda, double* x, int ldx, double* t, DeviceStatus* st,
-                                DescArena& arena, cudaStream_t s) {
+cudaError_t potrf_inverse_upper(int n, double* a, int lda, double* x, int ldx, double* t, unsigned* counter,
+                                int grid, DeviceStatus* st, uint64_t limit_ns, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  cudaError_t err = cudaFuncSetAttribute(chol_inv_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kLeafSmem);
+  cudaError_t err = cudaFuncSetAttribute(potrf_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kSmemBytes);
   if (err != cudaSuccess) return err;
-  err = cudaMemsetAsync(x, 0, sizeof(double) * ((size_t)ldx * (n - 1) + n), s);
-  if (err != cudaSuccess) return err;
-  return chol_inv_rec(a, lda, x, ldx, t, n, 0, n, st, arena, s);
+  if ((err = cudaMemsetAsync(x, 0, sizeof(double) * ((size_t)ldx * (n - 1) + n), s)) != cudaSuccess) return err;
+  if ((err = cudaMemsetAsync(counter, 0, 64 * sizeof(unsigned), s)) != cudaSuccess) return err;
+  PotrfParams p{a, lda, x, ldx, t, n, counter, st, limit_ns};
+  const int nt = (n + NB - 1) / NB;
+  // Enough CTAs for the widest phase (the first trailing update), never more than co-resident (one per SM).
+  const int G = std::max(1, std::min(grid, std::max(2, nt * (nt - 1) / 2)));
+  void* args[] = {(void*)&p};
+  err = cudaLaunchCooperativeKernel((void*)potrf_persistent_kernel, dim3(G), dim3(kThreads), args, kSmemBytes, s);
+  note_launches();
+  return err;
 }
 
 }  // namespace xtbeig
