@@ -128,9 +128,11 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
   }
 
   T x[CPT], vn[CPT], vk[CPT], wk[CPT];
+  int own_q[CPT];  // local row index when this thread's column c is also a row of this CTA, else -1
 #pragma unroll
   for (int j = 0; j < CPT; ++j) {
     const int c = tid + j * NT;
+    own_q[j] = (c % G == cta) ? c / G : -1;
     x[j] = (n >= 1 && c < n - 1) ? p.afull[c + (size_t)(n - 1) * p.ldf] : T(0);
     vk[j] = wk[j] = vn[j] = T(0);
   }
@@ -164,9 +166,13 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
     if (xn2 == T(0)) {
       beta = alpha; tau = T(0); scale = T(0);
     } else {
-      T nrm = sqrt(alpha * alpha + xn2);
+      // beta = -sign(alpha) ||(alpha, x)||, tau = (beta - alpha)/beta = 1 + |alpha|/||.||: one reciprocal square
+      // root and one division on the column's critical path.
+      const T s2 = alpha * alpha + xn2;
+      const T rn = rsqrt(s2);
+      const T nrm = s2 * rn;
       beta = alpha >= T(0) ? -nrm : nrm;
-      tau = (beta - alpha) / beta;
+      tau = T(1) + fabs(alpha) * rn;
       scale = T(1) / (alpha - beta);
     }
 #pragma unroll
@@ -203,11 +209,11 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
             if (c < k) {
               T a = row[c];
               if (has_prev) {
-                a -= vr * wk[j] + wr * vk[j];
+                a = fma(-vr, wk[j], a);
+                a = fma(-wr, vk[j], a);
                 row[c] = a;
               }
-              acc[qq] += a * vn[j];
-              if (c == k - 1) colk[q] = a;
+              acc[qq] = fma(a, vn[j], acc[qq]);
             }
           }
         }
@@ -215,6 +221,14 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
       const T rs = warp_reduce_scatter8(acc);
       const int qrow = q0 + ((lane >> 2) & 7);
       if ((lane & 3) == 0 && qrow < R) red[qrow * NW + warp] = rs;
+    }
+    // A(r, k-1) after the update, for the next column: the thread that owns column k-1 (and just wrote it) reads it
+    // back, so the element loop above carries no per-element test for it.
+    if (tid == tk) {
+      for (int q = 0; q < R; ++q) {
+        if (cta + q * G >= k) break;
+        colk[q] = rows[q * ldr + (k - 1)];
+      }
     }
     __syncthreads();
     // ---- 3. publish (y_r, A(r,k-1)) for own rows, then read every row's pair for this thread's columns.
@@ -256,10 +270,9 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
       x[j] = c < k - 1 ? colj[j] - vn[j] * wkm1 - w : T(0);
       vk[j] = vn[j];
       wk[j] = w;
-      if (c < k && (c % G) == cta) {
-        const int q = c / G;
-        vrow[q] = vn[j];
-        wrow[q] = w;
+      if (c < k && own_q[j] >= 0) {
+        vrow[own_q[j]] = vn[j];
+        wrow[own_q[j]] = w;
       }
     }
   }
