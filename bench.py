@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0, help="bound on the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-count", type=int, default=256, help="uneven batch size (0: skip the batch section)")
+    ap.add_argument("--batch-steps", type=int, default=3)
     return ap.parse_args()
 
 
@@ -186,6 +188,150 @@ def load_traffic(n):
     return float(rec["bytes_per_launch"]) * (n / rec["n"]) ** 3 if rec.get("n") else None
 
 
+def generalized_on_device(n, seed, dev):
+    """The generalized construction (S = I + banded random G shifted to lambda_min >= 0.05, lam ~ U[-1, 0.5] Eh with a
+    0.05 Eh gap at n/2, H = S^1/2 Q diag(lam) Q^T S^1/2) built on the GPU with torch's generator seeded `seed`: same
+    distribution as the host builder (numpy's generator differs), used to make the 256 batch problems quickly.  The
+    exact generalized spectrum is lam.  Input generation only, never timed."""
+    import torch
+
+    f64 = torch.float64
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    idx = torch.arange(n, device=dev, dtype=f64)
+    dist = (idx[:, None] - idx[None, :]).abs()
+    u = torch.rand((n, n), generator=g, device=dev, dtype=f64) * 2.0 - 1.0
+    gm = 0.35 * torch.exp(-dist / 12.0) * torch.triu(u, 1)
+    eye = torch.eye(n, device=dev, dtype=f64)
+    s = eye + gm + gm.T
+    lmin = float(torch.linalg.eigvalsh(s)[0])
+    if lmin < 0.05:
+        s += (0.05 - lmin) * eye
+    lam = torch.sort(torch.rand(n, generator=g, device=dev, dtype=f64) * 1.5 - 1.0).values
+    lam[n // 2:] += 0.05
+    q, r = torch.linalg.qr(torch.randn((n, n), generator=g, device=dev, dtype=f64))
+    q = q * torch.sign(torch.diagonal(r))[None, :]
+    ws, vs = torch.linalg.eigh(s)
+    shalf = (vs * torch.sqrt(ws)[None, :]) @ vs.T
+    shalf = 0.5 * (shalf + shalf.T)
+    h = shalf @ ((q * lam[None, :]) @ q.T) @ shalf
+    h = 0.5 * (h + h.T)
+    return h.contiguous(), s.contiguous(), lam
+
+
+def run_batch_section(args, dev, stream):
+    """The uneven batch: `count` generalized problems, sizes U[124, 1788] (seed 3), problem i built with seed
+    1000 + i.  Device-resident batches through xtb_dsygvd_batched_device (restore of H, S inside each timed step),
+    the same problems solved one at a time through xtb_dsygvd_device (per-size times), and one end-to-end batch
+    through xtb_dsygvd_batched from pinned host arrays."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import xtbeig
+    from oracle import inputs
+
+    count = args.batch_count
+    sizes = inputs.batch_sizes(count, seed=3)
+    t0 = time.perf_counter()
+    H0, S0, LAM = [], [], []
+    for i, n in enumerate(sizes):
+        h, s, lam = generalized_on_device(n, 1000 + i, dev)
+        H0.append(h)
+        S0.append(s)
+        LAM.append(lam)
+    torch.cuda.synchronize(dev)
+    gen_s = time.perf_counter() - t0
+    H = [torch.empty_like(x) for x in H0]
+    S = [torch.empty_like(x) for x in S0]
+    W = [torch.empty(n, dtype=torch.float64, device=dev) for n in sizes]
+    hp, sp, wp = [x.data_ptr() for x in H], [x.data_ptr() for x in S], [x.data_ptr() for x in W]
+
+    def batch_step():
+        for i in range(count):
+            H[i].copy_(H0[i])
+            S[i].copy_(S0[i])
+        info, r = xtbeig.dsygvd_batched_device(sizes, hp, sizes, sp, sizes, wp, stream.cuda_stream)
+        if r != 0:
+            raise RuntimeError(f"xtb_dsygvd_batched_device returned {r}: {xtbeig.last_error()}")
+
+    workers = xtbeig.get_option("batch_workers")
+    for _ in range(3):  # eager, captured, replayed
+        batch_step()
+    torch.cuda.synchronize(dev)
+    steps = max(1, args.batch_steps)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    launches0 = xtbeig.launch_count()
+    for k in range(steps):
+        ev[k][0].record(stream)
+        batch_step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    launches = xtbeig.launch_count() - launches0
+    ms_batch = statistics.mean(a.elapsed_time(b) for a, b in ev)
+    eig_err = max(float((W[i] - LAM[i]).abs().max()) for i in range(count))
+
+    # One at a time: each problem alone on the caller's stream (eager, captured, then the timed replay).
+    per = []
+    for i, n in enumerate(sizes):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for rep in range(3):
+            H[i].copy_(H0[i])
+            S[i].copy_(S0[i])
+            if rep == 2:
+                e0.record(stream)
+            info = xtbeig.dsygvd_device(n, hp[i], n, sp[i], n, wp[i], stream.cuda_stream)
+            if info != 0:
+                raise RuntimeError(f"xtb_dsygvd_device info={info}: {xtbeig.last_error()}")
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        per.append(e0.elapsed_time(e1))
+    one_ms = sum(per)
+    bins = {}
+    for lo, hi in ((124, 500), (500, 900), (900, 1300), (1300, 1789)):
+        sel = [t for n, t in zip(sizes, per) if lo <= n < hi]
+        if sel:
+            bins[f"{lo}-{hi - 1}"] = {"count": len(sel), "mean_ms_alone": round(statistics.mean(sel), 3)}
+
+    # End to end through the host C ABI: pinned host H, S in, C, U, w back.
+    L = xtbeig.lib()
+    hh = [torch.empty((n, n), dtype=torch.float64, pin_memory=True) for n in sizes]
+    sh = [torch.empty((n, n), dtype=torch.float64, pin_memory=True) for n in sizes]
+    wh = [torch.empty(n, dtype=torch.float64, pin_memory=True) for n in sizes]
+    ns = np.array(sizes, np.int32)
+    ap = (ctypes.c_void_p * count)(*[x.data_ptr() for x in hh])
+    bp = (ctypes.c_void_p * count)(*[x.data_ptr() for x in sh])
+    wq = (ctypes.c_void_p * count)(*[x.data_ptr() for x in wh])
+    infos = np.zeros(count, np.int32)
+    e2e = []
+    for rep in range(2):
+        for i in range(count):
+            hh[i].copy_(H0[i])
+            sh[i].copy_(S0[i])
+        t1 = time.perf_counter()
+        r = L.xtb_dsygvd_batched(count, xtbeig._p(ns), ap, xtbeig._p(ns), bp, xtbeig._p(ns), wq, xtbeig._p(infos))
+        dt = time.perf_counter() - t1
+        if r != 0:
+            raise RuntimeError(f"xtb_dsygvd_batched returned {r}: {xtbeig.last_error()}")
+        if rep == 1:
+            e2e.append(dt)
+    elems = sum(n * n for n in sizes)
+    return {
+        "count": count, "sizes": "uniform integers in [124, 1788], seed 3; problem i built with seed 1000 + i",
+        "workers": workers, "solves_per_s": round(count / (ms_batch * 1e-3), 2), "ms_per_batch": round(ms_batch, 2),
+        "steps": steps, "warmup": 3, "gpu_launches_per_batch": int(launches // steps),
+        "one_at_a_time_solves_per_s": round(count / (one_ms * 1e-3), 2), "one_at_a_time_ms": round(one_ms, 2),
+        "speedup_vs_one_at_a_time": round(one_ms / ms_batch, 3), "per_size_ms_alone": bins,
+        "eigenvalue_error_vs_exact_max": eig_err,
+        "e2e": {"solves_per_s": round(count / e2e[0], 2), "ms_per_batch": round(e2e[0] * 1e3, 2),
+                "h2d_bytes_per_batch": 2 * elems * 8, "d2h_bytes_per_batch": (2 * elems + sum(sizes)) * 8},
+        "l2": "not flushed: the batch's matrices (~%.1f GB) exceed L2" % (4 * elems * 8 / 1e9),
+        "input_generation_s": round(gen_s, 1),
+        "input_builder": "torch on the device (generator seeded per problem), outside every timed region",
+    }
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -293,6 +439,8 @@ def run_ours(args):
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_ms = float(te.item())
 
+    batch = run_batch_section(args, dev, stream) if args.batch_count > 0 else None
+
     if rank == 0:
         peak, peak_kind = load_peaks()
         t_sytrd = dict(stages).get("sytrd")
@@ -327,6 +475,7 @@ def run_ours(args):
                     "per_replica_ms": round(e2e_ms, 4)},
             "gpu_launches": int(launches),
             "clocks": clocks,
+            "batch": batch,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

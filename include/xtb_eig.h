@@ -88,10 +88,20 @@ int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, 
 int xtb_dsytrd_upper_noalloc(int n, double* a, int lda, double* d, double* e, double* tau, void* stream);
 
 /* A batch of independent generalized problems (host arrays, itype 1, jobz 'V', uplo 'U'): problem i has size n[i],
- * a[i] (lda[i]), b[i] (ldb[i]), w[i]; info[i] per problem.  Problems are ordered by n^3 (longest first) and spread
- * over the library's streams.  Returns 0 or the first nonzero info. */
+ * a[i] (lda[i]), b[i] (ldb[i]), w[i]; info[i] per problem (info may be NULL).  The problems are assigned to the
+ * library's worker threads longest first (static LPT on a cost model of n), each worker with its own stream and
+ * workspace, so that problems overlap on the GPU; results equal the single-problem call's bit for bit.  Returns 0,
+ * the info of the lowest-numbered failing problem (whose message becomes xtb_gpu_last_error()), -1 for count < 0, or
+ * -2 for a NULL array or an n/lda/ldb that is invalid for some problem (nothing is computed then).  Option
+ * "batch_workers" sets the number of workers. */
 int xtb_dsygvd_batched(int count, const int* n, double* const* a, const int* lda, double* const* b, const int* ldb,
                        double* const* w, int* info);
+/* The same on DEVICE pointers (a[i], b[i], w[i] in device memory of the current device; the pointer arrays and n,
+ * lda, ldb, info on the host).  Work queued on `stream` (NULL: the legacy default stream) before the call is finished
+ * before any problem starts; the call returns when every problem has finished.  A batch repeated on the same buffers
+ * replays each worker's captured graphs from its third call on (option "graphs"). */
+int xtb_dsygvd_batched_device(int count, const int* n, double* const* a, const int* lda, double* const* b,
+                              const int* ldb, double* const* w, int* info, void* stream);
 
 /* Adjoint of the Fermi-smeared density matrix P = C diag(f) C^T, f_i = 2 / (1 + exp((e_i - mu)/kT)), where
  * H C = S C diag(e), C^T S C = I (H, S upper triangles, host arrays).  Given dL/dP = wbar (symmetric, n x n), returns
@@ -104,7 +114,8 @@ int xtb_dsygvd_density_adjoint(int n, const double* h, int ldh, const double* s,
 /* Options (process-wide): "sytrd_grid" (CTAs of the resident reduction, 0 = auto), "ormtr_nb" (reflectors per
  * compact-WY block, default 128), "wait_limit_ms" (device wait time limit, default 2000), "stage_timing" (1: record
  * CUDA events at stage boundaries; read with xtb_gpu_stage_*), "graphs" (default 1: a device-pointer solve repeated
- * on the same buffers and non-NULL stream is captured into a CUDA graph on its second call and replayed after).
+ * on the same buffers and non-NULL stream is captured into a CUDA graph on its second call and replayed after),
+ * "batch_workers" (host threads, each with its own stream, that the batch calls spread problems over; default 4).
  * Returns 0, or -1 for an unknown name. */
 int xtb_gpu_set_option(const char* name, long value);
 long xtb_gpu_get_option(const char* name);

@@ -121,14 +121,101 @@ def test_density_adjoint_matches_dk_oracle(xe, temp):
     assert np.max(np.abs(ds - gs)) < 1e-9 * scale_s
 
 
-def test_batched_uneven(xe):
-    sizes = [37, 130, 64, 9, 200]
-    probs = [inputs.generalized(n, seed=1000 + i) for i, n in enumerate(sizes)]
-    w, c, u, info = xe.dsygvd_batched([p[0] for p in probs], [p[1] for p in probs])
-    assert np.all(info == 0)
-    for (h, s, lam), wi, ci in zip(probs, w, c):
+def _batch_problems(sizes, seed0=1000):
+    return [inputs.generalized(n, seed=seed0 + i) for i, n in enumerate(sizes)]
+
+
+@pytest.mark.parametrize("workers", [1, 3, 4])
+def test_batched_uneven(xe, workers):
+    """Uneven batch (the batch configuration's construction at small sizes, an empty problem included): every
+    problem within the FP64 bars, and bit for bit the single-problem call's result whatever the worker count."""
+    sizes = [37, 130, 64, 9, 200, 0, 311, 1, 96]
+    probs = [inputs.generalized(n, seed=1000 + i) if n else (np.zeros((0, 0)), np.zeros((0, 0)), np.zeros(0))
+             for i, n in enumerate(sizes)]
+    old = xe.get_option("batch_workers")
+    xe.set_option("batch_workers", workers)
+    try:
+        w, c, u, info, ret = xe.dsygvd_batched([p[0] for p in probs], [p[1] for p in probs])
+    finally:
+        xe.set_option("batch_workers", old)
+    assert ret == 0 and np.all(info == 0)
+    for (h, s, lam), wi, ci, ui in zip(probs, w, c, u):
+        n = h.shape[0]
+        if n == 0:
+            continue
         assert np.max(np.abs(wi - lam)) < 1e-10
         assert metrics.backward_error(h, s, wi, ci) < 10
+        w1, c1, u1, info1 = xe.dsygvd(h, s)
+        assert info1 == 0
+        np.testing.assert_array_equal(wi, w1)
+        np.testing.assert_array_equal(ci, c1)
+        np.testing.assert_array_equal(np.triu(ui), np.triu(u1))
+
+
+def test_batched_failure_is_per_problem(xe):
+    """A non-SPD overlap in one problem fails that problem only (info = n + failing column, as dsygvd) and the call
+    returns its info; the other problems are solved."""
+    sizes = [80, 70, 120]
+    probs = _batch_problems(sizes, seed0=2000)
+    hs = [p[0] for p in probs]
+    ss = [p[1].copy() for p in probs]
+    ss[1][40, 40] = -1.0
+    _, info_ref = lapack.potrf_upper(ss[1])
+    w, c, u, info, ret = xe.dsygvd_batched(hs, ss)
+    assert info[1] == 70 + info_ref and info[0] == 0 and info[2] == 0
+    assert ret == info[1]
+    assert "problem 1" in xe.last_error()
+    for i in (0, 2):
+        assert np.max(np.abs(w[i] - probs[i][2])) < 1e-10
+
+
+def test_batched_invalid_arguments(xe):
+    import ctypes as C
+
+    lib = xe.lib()
+    ns = np.array([10, 5], np.int32)
+    lds = np.array([10, 4], np.int32)  # lda < n for problem 1
+    a = [np.zeros((10, 10), order="F"), np.zeros((5, 5), order="F")]
+    w = [np.zeros(10), np.zeros(5)]
+    ap = (C.c_void_p * 2)(*[x.ctypes.data for x in a])
+    wp = (C.c_void_p * 2)(*[x.ctypes.data for x in w])
+    info = np.zeros(2, np.int32)
+    assert lib.xtb_dsygvd_batched(2, ns.ctypes.data, ap, lds.ctypes.data, ap, ns.ctypes.data, wp,
+                                  info.ctypes.data) == -2
+    assert lib.xtb_dsygvd_batched(-1, ns.ctypes.data, ap, ns.ctypes.data, ap, ns.ctypes.data, wp,
+                                  info.ctypes.data) == -1
+    assert lib.xtb_dsygvd_batched(0, None, None, None, None, None, None, None) == 0
+
+
+def test_batched_device_repeated_graph_replay(xe):
+    """Device-pointer batch repeated on the same buffers (eager, captured, replayed): each call bit for bit the host
+    batch's result, and work queued on the caller's stream before the call (the input restore) is seen."""
+    import torch
+
+    sizes = [150, 61, 233, 90, 12]
+    probs = _batch_problems(sizes, seed0=3000)
+    w_ref, c_ref, u_ref, info_ref, ret = xe.dsygvd_batched([p[0] for p in probs], [p[1] for p in probs])
+    assert ret == 0
+    dev = torch.device("cuda", 0)
+    xe.set_device(0)
+    stream = torch.cuda.Stream(dev)
+    H0 = [torch.from_numpy(np.ascontiguousarray(p[0])).to(dev) for p in probs]
+    S0 = [torch.from_numpy(np.ascontiguousarray(p[1])).to(dev) for p in probs]
+    H = [torch.empty_like(x) for x in H0]
+    S = [torch.empty_like(x) for x in S0]
+    W = [torch.empty(n, dtype=torch.float64, device=dev) for n in sizes]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for _ in range(4):
+            for i in range(len(sizes)):
+                H[i].copy_(H0[i])
+                S[i].copy_(S0[i])
+            info, r = xe.dsygvd_batched_device(sizes, [x.data_ptr() for x in H], sizes, [x.data_ptr() for x in S],
+                                               sizes, [x.data_ptr() for x in W], stream.cuda_stream)
+            assert r == 0 and np.all(info == 0)
+            for i in range(len(sizes)):
+                np.testing.assert_array_equal(W[i].cpu().numpy(), w_ref[i])
+                np.testing.assert_array_equal(H[i].cpu().numpy().T, c_ref[i])
 
 
 @pytest.mark.parametrize("graphs", [0, 1])

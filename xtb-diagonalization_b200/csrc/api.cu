@@ -9,9 +9,12 @@
 #include <algorithm>
 #include <atomic>
 #include <cctype>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -27,7 +30,9 @@ std::atomic<long> g_ormtr_nb{128};
 std::atomic<long> g_wait_ms{2000};
 std::atomic<long> g_stage_timing{0};
 std::atomic<long> g_graphs{1};
+std::atomic<long> g_batch_workers{4};
 std::atomic<long long> g_launches{0};
+thread_local long long t_launches = 0;  // this thread's launches: a graph capture counts its own, not other threads'
 
 struct Buf {
   void* p = nullptr;
@@ -478,7 +483,7 @@ int run_graphed(Context* c, cudaStream_t s, const std::vector<long long>& key, D
   }
   if (graphs_on && ge.calls >= 1 && !ge.failed) {
     const uint64_t gen0 = c->generation;
-    const long long launches0 = g_launches.load();
+    const long long launches0 = t_launches;
     cudaError_t err = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (err == cudaSuccess) {
       {
@@ -487,8 +492,9 @@ int run_graphed(Context* c, cudaStream_t s, const std::vector<long long>& key, D
         err = k.err;
       }
       // Captured launches are not executed now: move them from the counter to the entry's per-replay count.
-      ge.kernels = g_launches.load() - launches0;
+      ge.kernels = t_launches - launches0;
       g_launches.fetch_sub(ge.kernels, std::memory_order_relaxed);
+      t_launches = launches0;
       cudaGraph_t graph = nullptr;
       const cudaError_t e2 = cudaStreamEndCapture(s, &graph);
       if (err == cudaSuccess && e2 == cudaSuccess && graph && c->generation == gen0) {
@@ -518,11 +524,199 @@ int run_graphed(Context* c, cudaStream_t s, const std::vector<long long>& key, D
 
 }  // namespace
 
-void note_launches(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+void note_launches(int k) {
+  g_launches.fetch_add(k, std::memory_order_relaxed);
+  t_launches += k;
+}
 
 }  // namespace xtbeig
 
 using namespace xtbeig;
+
+namespace {
+
+// dsygvd (itype 1, arguments already checked, n > 0) on the calling thread's context: host arrays in, results back.
+int sygvd_host(char jz, char ul, int n, double* a, int lda, double* b, int ldb, double* w) {
+  Context* c = context();
+  if (!c) return t_state.last_code;
+  Call k(c, nullptr);
+  double* da = k.dev<double>("io.A", (size_t)lda * n);
+  double* db = k.dev<double>("io.B", (size_t)ldb * n);
+  double* dh = k.dev<double>("io.F", (size_t)n * n);
+  double* du = k.dev<double>("io.U", (size_t)n * n);
+  double* dc = k.dev<double>("io.C", (size_t)n * n);
+  double* dw = k.dev<double>("io.w", n);
+  k.h2d(da, a, sizeof(double) * (size_t)lda * n, "H2D A");
+  k.h2d(db, b, sizeof(double) * (size_t)ldb * n, "H2D B");
+  if (k.ok()) {
+    if (ul == 'U') {
+      symmetrize_upper<double>(n, da, lda, dh, n, k.s);
+      copy_matrix<double>(n, n, db, ldb, du, n, k.s);
+    } else {
+      symmetrize_lower<double>(n, da, lda, dh, n, k.s);
+      symmetrize_lower<double>(n, db, ldb, du, n, k.s);
+    }
+  }
+  core_sygvd(k, n, dh, du, dc, dw);
+  // B <- the factor in the caller's triangle; the other triangle keeps its input (du's lower part is the input's).
+  if (k.ok()) {
+    if (ul == 'U') copy_matrix<double>(n, n, du, n, db, ldb, k.s);
+    else upper_transpose_to_lower<double>(n, du, n, db, ldb, k.s);
+  }
+  k.d2h(b, db, sizeof(double) * (size_t)ldb * n, "D2H B");
+  k.d2h(w, dw, sizeof(double) * n, "D2H w");
+  if (jz == 'V' && k.ok())
+    k.check(cudaMemcpy2DAsync(a, sizeof(double) * lda, dc, sizeof(double) * n, sizeof(double) * n, n,
+                              cudaMemcpyDeviceToHost, k.s), "D2H C");
+  DeviceStatus st{};
+  const int code = k.finish(&st);
+  return info_of(code, st, n);
+}
+
+// Device-pointer dsygvd body (upper triangles in a and b, ld lda/ldb): a <- C, b <- U, w <- eigenvalues.
+void sygvd_device_body(Call& k, int n, double* a, int lda, double* b, int ldb, double* w) {
+  double* dh = k.dev<double>("dv.F", (size_t)n * n);
+  double* du = k.dev<double>("dv.U", (size_t)n * n);
+  double* dc = k.dev<double>("dv.C", (size_t)n * n);
+  if (k.ok()) {
+    symmetrize_upper<double>(n, a, lda, dh, n, k.s);
+    copy_matrix<double>(n, n, b, ldb, du, n, k.s);
+  }
+  core_sygvd(k, n, dh, du, dc, w);
+  if (k.ok()) {
+    copy_matrix<double>(n, n, dc, n, a, lda, k.s);
+    copy_matrix<double>(n, n, du, n, b, ldb, k.s);
+  }
+}
+
+int sygvd_device(Context* c, cudaStream_t s, int n, double* a, int lda, double* b, int ldb, double* w) {
+  const std::vector<long long> key = {1, n, (long long)(uintptr_t)a, lda, (long long)(uintptr_t)b, ldb,
+                                      (long long)(uintptr_t)w, (long long)(uintptr_t)s};
+  DeviceStatus st{};
+  const int code = run_graphed(c, s, key, &st, [&](Call& k) { sygvd_device_body(k, n, a, lda, b, ldb, w); });
+  return info_of(code, st, n);
+}
+
+// Persistent host threads for batched solves.  Each worker keeps its own per-thread contexts (non-blocking stream,
+// workspace, captured graphs), so the problems of different workers run concurrently on the GPU: the persistent
+// reduction of a small problem occupies a fraction of the SMs, and one worker's barrier waits and launch gaps are
+// filled by the others' kernels.  Created on first use and never destroyed (idle threads wait on a condition).
+class WorkerPool {
+ public:
+  // Runs fn(w) for w = 0..nw-1, one per worker thread, and returns when all have returned.  Batches from several
+  // host threads are serialised.
+  void run(int nw, const std::function<void(int)>& fn) {
+    std::lock_guard<std::mutex> serial(call_mu_);
+    std::unique_lock<std::mutex> lk(mu_);
+    while (threads_ < nw) {
+      std::thread(&WorkerPool::loop, this, threads_).detach();
+      threads_++;
+    }
+    job_ = &fn;
+    active_ = nw;
+    remaining_ = nw;
+    epoch_++;
+    work_cv_.notify_all();
+    done_cv_.wait(lk, [&] { return remaining_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  void loop(int id) {
+    uint64_t seen = 0;
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      work_cv_.wait(lk, [&] { return epoch_ != seen; });
+      seen = epoch_;
+      if (id >= active_) continue;
+      const std::function<void(int)>* fn = job_;
+      lk.unlock();
+      (*fn)(id);
+      lk.lock();
+      if (--remaining_ == 0) done_cv_.notify_all();
+    }
+  }
+  std::mutex call_mu_, mu_;
+  std::condition_variable work_cv_, done_cv_;
+  const std::function<void(int)>* job_ = nullptr;
+  int threads_ = 0, active_ = 0, remaining_ = 0;
+  uint64_t epoch_ = 0;
+};
+
+WorkerPool& pool() {
+  static WorkerPool* p = new WorkerPool();
+  return *p;
+}
+
+// Static longest-processing-time assignment: problems in decreasing cost, each to the worker with the least assigned
+// cost so far.  The cost model follows the pipeline's measured shape: a per-column latency term (the resident
+// reduction and the divide-and-conquer levels advance one column or level at a time) plus an n^3 term for the
+// GEMM-shaped stages.  The same sizes always give the same assignment, so per-worker captured graphs replay.
+std::vector<std::vector<int>> lpt_assign(int count, const int* n, int nw) {
+  auto cost = [](int m) { return 5.0 * m + 1.3e-6 * (double)m * m * m; };  // microseconds
+  std::vector<int> order(count);
+  for (int i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return n[x] > n[y]; });
+  std::vector<std::vector<int>> lists(nw);
+  std::vector<double> load(nw, 0.0);
+  for (int i : order) {
+    int best = 0;
+    for (int w = 1; w < nw; ++w)
+      if (load[w] < load[best]) best = w;
+    lists[best].push_back(i);
+    load[best] += cost(n[i]);
+  }
+  return lists;
+}
+
+// Runs solve(i) for every problem on the worker pool; info[i] per problem.  Returns 0 or the info of the
+// lowest-numbered failing problem, whose message becomes the calling thread's last error.
+int run_batch(int count, const int* n, int* info, const std::function<int(int)>& solve) {
+  int dev = 0;
+  const cudaError_t derr = cudaGetDevice(&dev);
+  if (derr != cudaSuccess) {
+    record(-1000 - (int)derr, std::string("no CUDA device: ") + cudaGetErrorString(derr));
+    return -1000 - (int)derr;
+  }
+  const int nw = (int)std::max<long>(1, std::min<long>(std::min<long>(g_batch_workers.load(), 64), count));
+  const std::vector<std::vector<int>> lists = lpt_assign(count, n, nw);
+  std::vector<int> inf(count, 0);
+  std::vector<std::string> msg(count);
+  pool().run(nw, [&](int wk) {
+    const cudaError_t e = cudaSetDevice(dev);
+    for (int i : lists[wk]) {
+      if (e != cudaSuccess) {
+        inf[i] = -1000 - (int)e;
+        msg[i] = std::string("worker cudaSetDevice failed: ") + cudaGetErrorString(e);
+        continue;
+      }
+      inf[i] = solve(i);
+      if (inf[i] != 0) msg[i] = t_state.last_msg;
+    }
+  });
+  int first = 0;
+  for (int i = 0; i < count; ++i) {
+    if (info) info[i] = inf[i];
+    if (inf[i] != 0 && first == 0) {
+      first = inf[i];
+      record(inf[i], "problem " + std::to_string(i) + ": " + msg[i]);
+    }
+  }
+  if (first == 0) record(0, "");
+  return first;
+}
+
+int check_batch(int count, const int* n, const void* a, const int* lda, const void* b, const int* ldb,
+                const void* w) {
+  if (count < 0) return -1;
+  if (count == 0) return 0;
+  if (!n || !a || !lda || !b || !ldb || !w) return -2;
+  for (int i = 0; i < count; ++i)
+    if (n[i] < 0 || lda[i] < std::max(1, n[i]) || ldb[i] < std::max(1, n[i])) return -2;
+  return 0;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -639,40 +833,7 @@ void xtb_dsygvd_gpu(const int* itype, const char* jobz, const char* uplo, const 
   if (lda < std::max(1, n)) { *info = -6; return; }
   if (ldb < std::max(1, n)) { *info = -8; return; }
   if (n == 0) return;
-  Context* c = context();
-  if (!c) { *info = t_state.last_code; return; }
-  Call k(c, nullptr);
-  double* da = k.dev<double>("io.A", (size_t)lda * n);
-  double* db = k.dev<double>("io.B", (size_t)ldb * n);
-  double* dh = k.dev<double>("io.F", (size_t)n * n);
-  double* du = k.dev<double>("io.U", (size_t)n * n);
-  double* dc = k.dev<double>("io.C", (size_t)n * n);
-  double* dw = k.dev<double>("io.w", n);
-  k.h2d(da, a, sizeof(double) * (size_t)lda * n, "H2D A");
-  k.h2d(db, b, sizeof(double) * (size_t)ldb * n, "H2D B");
-  if (k.ok()) {
-    if (ul == 'U') {
-      symmetrize_upper<double>(n, da, lda, dh, n, k.s);
-      copy_matrix<double>(n, n, db, ldb, du, n, k.s);
-    } else {
-      symmetrize_lower<double>(n, da, lda, dh, n, k.s);
-      symmetrize_lower<double>(n, db, ldb, du, n, k.s);
-    }
-  }
-  core_sygvd(k, n, dh, du, dc, dw);
-  // B <- the factor in the caller's triangle; the other triangle keeps its input (du's lower part is the input's).
-  if (k.ok()) {
-    if (ul == 'U') copy_matrix<double>(n, n, du, n, db, ldb, k.s);
-    else upper_transpose_to_lower<double>(n, du, n, db, ldb, k.s);
-  }
-  k.d2h(b, db, sizeof(double) * (size_t)ldb * n, "D2H B");
-  k.d2h(w, dw, sizeof(double) * n, "D2H w");
-  if (jz == 'V' && k.ok())
-    k.check(cudaMemcpy2DAsync(a, sizeof(double) * lda, dc, sizeof(double) * n, sizeof(double) * n, n,
-                              cudaMemcpyDeviceToHost, k.s), "D2H C");
-  DeviceStatus st{};
-  int code = k.finish(&st);
-  *info = info_of(code, st, n);
+  *info = sygvd_host(jz, ul, n, a, lda, b, ldb, w);
 }
 
 
@@ -702,43 +863,45 @@ int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, 
   if (n == 0) return 0;
   Context* c = context();
   if (!c) return t_state.last_code;
-  const std::vector<long long> key = {1, n, (long long)(uintptr_t)a, lda, (long long)(uintptr_t)b, ldb,
-                                      (long long)(uintptr_t)w, (long long)(uintptr_t)stream};
-  DeviceStatus st{};
-  const int code = run_graphed(c, (cudaStream_t)stream, key, &st, [&](Call& k) {
-    double* dh = k.dev<double>("dv.F", (size_t)n * n);
-    double* du = k.dev<double>("dv.U", (size_t)n * n);
-    double* dc = k.dev<double>("dv.C", (size_t)n * n);
-    if (k.ok()) {
-      symmetrize_upper<double>(n, a, lda, dh, n, k.s);
-      copy_matrix<double>(n, n, b, ldb, du, n, k.s);
-    }
-    core_sygvd(k, n, dh, du, dc, w);
-    if (k.ok()) {
-      copy_matrix<double>(n, n, dc, n, a, lda, k.s);
-      copy_matrix<double>(n, n, du, n, b, ldb, k.s);
-    }
-  });
-  return info_of(code, st, n);
+  return sygvd_device(c, (cudaStream_t)stream, n, a, lda, b, ldb, w);
 }
 
 int xtb_dsygvd_batched(int count, const int* n, double* const* a, const int* lda, double* const* b, const int* ldb,
                        double* const* w, int* info) {
-  if (count <= 0) return 0;
-  // Longest first (n^3), so the tail of the batch is short problems.
-  std::vector<int> order(count);
-  for (int i = 0; i < count; ++i) order[i] = i;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return n[x] > n[y]; });
-  int first = 0;
-  const int itype = 1;
-  for (int idx : order) {
-    int inf = 0;
-    xtb_dsygvd_gpu(&itype, "V", "U", &n[idx], a[idx], &lda[idx], b[idx], &ldb[idx], w[idx], nullptr, nullptr,
-                   nullptr, nullptr, &inf);
-    if (info) info[idx] = inf;
-    if (inf != 0 && first == 0) first = inf;
+  const int bad = check_batch(count, n, a, lda, b, ldb, w);
+  if (bad != 0 || count == 0) return bad;
+  return run_batch(count, n, info, [&](int i) {
+    return n[i] == 0 ? 0 : sygvd_host('V', 'U', n[i], a[i], lda[i], b[i], ldb[i], w[i]);
+  });
+}
+
+int xtb_dsygvd_batched_device(int count, const int* n, double* const* a, const int* lda, double* const* b,
+                              const int* ldb, double* const* w, int* info, void* stream) {
+  const int bad = check_batch(count, n, a, lda, b, ldb, w);
+  if (bad != 0 || count == 0) return bad;
+  // Work queued on `stream` before the call is complete before any problem starts: the workers' streams wait on an
+  // event recorded here.
+  cudaEvent_t ready = nullptr;
+  cudaError_t err = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+  if (err == cudaSuccess) err = cudaEventRecord(ready, (cudaStream_t)stream);
+  if (err != cudaSuccess) {
+    if (ready) cudaEventDestroy(ready);
+    record(-1000 - (int)err, std::string("batch set-up failed: ") + cudaGetErrorString(err));
+    return -1000 - (int)err;
   }
-  return first;
+  const int r = run_batch(count, n, info, [&](int i) {
+    if (n[i] == 0) return 0;
+    Context* c = context();
+    if (!c) return t_state.last_code;
+    const cudaError_t we = cudaStreamWaitEvent(c->stream, ready, 0);
+    if (we != cudaSuccess) {
+      record(-1000 - (int)we, std::string("stream wait failed: ") + cudaGetErrorString(we));
+      return -1000 - (int)we;
+    }
+    return sygvd_device(c, c->stream, n[i], a[i], lda[i], b[i], ldb[i], w[i]);
+  });
+  cudaEventDestroy(ready);
+  return r;
 }
 
 int xtb_dsygvd_density_adjoint(int n, const double* h, int ldh, const double* s, int lds, double kt, double mu,
@@ -804,6 +967,7 @@ int xtb_gpu_set_option(const char* name, long value) {
   if (!std::strcmp(name, "wait_limit_ms")) { g_wait_ms = value; return 0; }
   if (!std::strcmp(name, "stage_timing")) { g_stage_timing = value; return 0; }
   if (!std::strcmp(name, "graphs")) { g_graphs = value; return 0; }
+  if (!std::strcmp(name, "batch_workers")) { g_batch_workers = value; return 0; }
   return -1;
 }
 
@@ -814,6 +978,7 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "wait_limit_ms")) return g_wait_ms;
   if (!std::strcmp(name, "stage_timing")) return g_stage_timing;
   if (!std::strcmp(name, "graphs")) return g_graphs;
+  if (!std::strcmp(name, "batch_workers")) return g_batch_workers;
   return -1;
 }
 

@@ -46,6 +46,7 @@ def lib():
         _lib.xtb_dsygvd_density_adjoint.argtypes = [_I, _P, _I, _P, _I, C.c_double, C.c_double, _P, _I, _P, _I, _P,
                                                     _I, _P, _P, _I]
         _lib.xtb_dsygvd_batched.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P]
+        _lib.xtb_dsygvd_batched_device.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P]
         _lib.xtb_gpu_stage_name.restype = C.c_char_p
         _lib.xtb_gpu_stage_name.argtypes = [_I]
         _lib.xtb_gpu_stage_ms.restype = C.c_double
@@ -219,18 +220,34 @@ def dsyevd_device(n, a_ptr, lda, w_ptr, stream=0) -> int:
 
 
 def dsygvd_batched(hs, ss):
-    """Batch of generalized problems; returns lists (w_i, C_i, U_i) and the info array."""
+    """Batch of generalized problems; returns lists (w_i, C_i, U_i), the info array and the call's return value."""
     count = len(hs)
     a = [np.array(h, dtype=np.float64, order="F", copy=True) for h in hs]
     b = [np.array(s, dtype=np.float64, order="F", copy=True) for s in ss]
     ns = np.array([x.shape[0] for x in a], np.int32)
-    w = [np.zeros(x.shape[0]) for x in a]
+    w = [np.zeros(max(x.shape[0], 1)) for x in a]
     ap = (C.c_void_p * count)(*[x.ctypes.data for x in a])
     bp = (C.c_void_p * count)(*[x.ctypes.data for x in b])
     wp = (C.c_void_p * count)(*[x.ctypes.data for x in w])
     info = np.zeros(count, np.int32)
-    lib().xtb_dsygvd_batched(count, _p(ns), ap, _p(ns), bp, _p(ns), wp, _p(info))
-    return w, a, b, info
+    ld = np.maximum(ns, 1).astype(np.int32)
+    ret = lib().xtb_dsygvd_batched(count, _p(ns), ap, _p(ld), bp, _p(ld), wp, _p(info))
+    return [x[:m] for x, m in zip(w, ns)], a, b, info, int(ret)
+
+
+def dsygvd_batched_device(ns, a_ptrs, ldas, b_ptrs, ldbs, w_ptrs, stream=0):
+    """Device-pointer batch: ns, ldas, ldbs int sequences, *_ptrs device addresses.  Returns (info array, ret)."""
+    count = len(ns)
+    ns = np.asarray(ns, np.int32)
+    ldas = np.asarray(ldas, np.int32)
+    ldbs = np.asarray(ldbs, np.int32)
+    ap = (C.c_void_p * count)(*[int(x) for x in a_ptrs])
+    bp = (C.c_void_p * count)(*[int(x) for x in b_ptrs])
+    wp = (C.c_void_p * count)(*[int(x) for x in w_ptrs])
+    info = np.zeros(count, np.int32)
+    ret = lib().xtb_dsygvd_batched_device(count, _p(ns), ap, _p(ldas), bp, _p(ldbs), wp, _p(info),
+                                          _P(stream) if stream else None)
+    return info, int(ret)
 
 
 def density_adjoint(h, s, kt, mu, wbar):
