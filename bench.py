@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-count", type=int, default=256, help="uneven batch size (0: skip the batch section)")
     ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision section")
     return ap.parse_args()
 
 
@@ -219,6 +220,78 @@ def generalized_on_device(n, seed, dev):
     return h.contiguous(), s.contiguous(), lam
 
 
+def accuracy_on_device(H, S, lam, C, w, C_ref):
+    """Errors of (w, C) for H C = S C diag(w) (torch float64 on the device, C column vectors): eigenvalues against
+    the exact spectrum lam, backward error ||HC - SC diag(w)||_F / (||H||_F n eps), S-orthogonality max|C^T S C - I|,
+    and the aufbau density (2 electrons in the lower half) against C_ref's.  Measurement only (torch matmuls)."""
+    import torch
+
+    n = H.shape[0]
+    eps = 2.0 ** -53
+    r = H @ C - (S @ C) * w[None, :]
+    bwd = float(torch.linalg.norm(r) / (torch.linalg.norm(H) * n * eps))
+    orth = float((C.T @ S @ C - torch.eye(n, dtype=C.dtype, device=C.device)).abs().max())
+    m = n // 2
+    p = 2.0 * C[:, :m] @ C[:, :m].T
+    p_ref = 2.0 * C_ref[:, :m] @ C_ref[:, :m].T
+    return {"eigenvalue_error_vs_exact": float((w - lam).abs().max()), "backward_error": bwd,
+            "s_orthogonality": orth, "density_error_vs_fp64_gpu": float((p - p_ref).abs().max())}
+
+
+def run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush):
+    """The same n = 1788 solve with precision 32: FP32 congruence, resident sytrd, ormtr and back-transform (FP64
+    Cholesky and tridiagonal eigensolve), then FP64 refinement (two Ogita-Aishima steps) on the FP64 pair.  Timed like
+    the FP64 path; accuracy against the exact spectrum and the FP64 GPU result."""
+    import torch
+
+    import xtbeig
+
+    n = H0.shape[0]
+    H, S = torch.empty_like(H0), torch.empty_like(S0)
+    W = torch.empty(n, dtype=torch.float64, device=dev)
+
+    def solve():
+        H.copy_(H0)
+        S.copy_(S0)
+        info = xtbeig.dsygvd_device(n, H.data_ptr(), n, S.data_ptr(), n, W.data_ptr(), stream.cuda_stream)
+        if info != 0:
+            raise RuntimeError(f"mixed xtb_dsygvd_device info={info}: {xtbeig.last_error()}")
+
+    xtbeig.set_option("precision", 32)
+    try:
+        for _ in range(3):
+            solve()
+        torch.cuda.synchronize(dev)
+        acc = accuracy_on_device(H0, S0, lam_t, H.T, W, C64)
+        xtbeig.set_option("stage_timing", 1)
+        flush.zero_()
+        solve()
+        stages = xtbeig.stage_times()
+        xtbeig.set_option("stage_timing", 0)
+        K = max(1, args.steps // 2)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        for i in range(K):
+            flush.zero_()
+            ev[i][0].record(stream)
+            solve()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+        ms = sum(a.elapsed_time(b) for a, b in ev) / K
+    finally:
+        xtbeig.set_option("precision", 64)
+    out = {"ms": round(ms, 4), "steps": K, "warmup": 3, "refine_iters": xtbeig.get_option("refine_iters"),
+           "stages_ms": {k: round(v, 4) for k, v in stages}}
+    out.update(acc)
+    return out
+
+
+def batch_sizes(count, seed=3, lo=124, hi=1788):
+    """Sizes of the uneven batch: integers uniform in [lo, hi] from numpy's default_rng(seed)."""
+    import numpy as np
+
+    return [int(x) for x in np.random.default_rng(seed).integers(lo, hi + 1, count)]
+
+
 def run_batch_section(args, dev, stream):
     """The uneven batch: `count` generalized problems, sizes U[124, 1788] (seed 3), problem i built with seed
     1000 + i.  Device-resident batches through xtb_dsygvd_batched_device (restore of H, S inside each timed step),
@@ -230,10 +303,9 @@ def run_batch_section(args, dev, stream):
     import torch
 
     import xtbeig
-    from oracle import inputs
 
     count = args.batch_count
-    sizes = inputs.batch_sizes(count, seed=3)
+    sizes = batch_sizes(count, seed=3)
     t0 = time.perf_counter()
     H0, S0, LAM = [], [], []
     for i, n in enumerate(sizes):
@@ -338,7 +410,6 @@ def run_ours(args):
     import torch.distributed as dist
 
     import xtbeig
-    from oracle import inputs
 
     rank, local_rank, world = rank_info()
     if world > 1:
@@ -349,11 +420,11 @@ def run_ours(args):
     xtbeig.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     n = args.n
-    h_np, s_np, lam = inputs.generalized(n, seed=args.seed + rank * 0)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
-    H0 = torch.from_numpy(np.ascontiguousarray(h_np)).to(dev)  # symmetric: row-major == column-major
-    S0 = torch.from_numpy(np.ascontiguousarray(s_np)).to(dev)
+    H0, S0, lam_t = generalized_on_device(n, args.seed, dev)  # symmetric: row-major == column-major
+    lam = lam_t.cpu().numpy()
+    h_np, s_np = H0.cpu().numpy(), S0.cpu().numpy()
     H = torch.empty_like(H0)
     S = torch.empty_like(S0)
     W = torch.empty(n, dtype=torch.float64, device=dev)
@@ -372,6 +443,8 @@ def run_ours(args):
     # accuracy of the measured configuration (outside the timed region)
     w = W.cpu().numpy()
     eig_err = float(np.max(np.abs(w - lam)))
+    C64 = H.T.contiguous()
+    acc64 = accuracy_on_device(H0, S0, lam_t, C64, W.clone(), C64)
 
     # Stage times of one untimed solve (CUDA events at stage boundaries inside the library).
     xtbeig.set_option("stage_timing", 1)
@@ -439,6 +512,9 @@ def run_ours(args):
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_ms = float(te.item())
 
+    mixed = run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush) if not args.no_mixed else None
+    if mixed:
+        mixed["speedup_vs_fp64"] = round(ms_step_max / mixed["ms"], 3)
     batch = run_batch_section(args, dev, stream) if args.batch_count > 0 else None
 
     if rank == 0:
@@ -475,6 +551,8 @@ def run_ours(args):
                     "per_replica_ms": round(e2e_ms, 4)},
             "gpu_launches": int(launches),
             "clocks": clocks,
+            "fp64_accuracy": acc64,
+            "mixed": mixed,
             "batch": batch,
         }
         print(json.dumps(line), flush=True)

@@ -87,6 +87,15 @@ int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, 
 #define XTB_NOALLOC_MAX_N 1792
 int xtb_dsytrd_upper_noalloc(int n, double* a, int lda, double* d, double* e, double* tau, void* stream);
 
+/* FP64 refinement of an approximate generalized eigendecomposition on DEVICE pointers: h, s (upper triangles, ldh,
+ * lds), c (n x n, ldc) approximate eigenvectors in ascending eigenvalue order (e.g. an FP32 solve, or the previous
+ * SCC cycle's C), w receives the eigenvalues.  `iters` Ogita-Aishima steps in the S inner product (the reference's refinement,
+ * scripts/kernels/refine.f90:258-325, with S in place of the identity; clusters of eigenvalues closer than delta =
+ * clamp(32 max|C^T H C|_offdiag, 1e-10, 1e-3) solved exactly within their block), then c, w in ascending order.
+ * Returns 0, -1000 - cudaError, or -(argument position) for an invalid argument (iters in 1..10). */
+int xtb_dsygvd_refine_device(int n, const double* h, int ldh, const double* s, int lds, double* c, int ldc,
+                             double* w, int iters, void* stream);
+
 /* A batch of independent generalized problems (host arrays, itype 1, jobz 'V', uplo 'U'): problem i has size n[i],
  * a[i] (lda[i]), b[i] (ldb[i]), w[i]; info[i] per problem (info may be NULL).  The problems are assigned to the
  * library's worker threads longest first (static LPT on a cost model of n), each worker with its own stream and
@@ -115,8 +124,11 @@ int xtb_dsygvd_density_adjoint(int n, const double* h, int ldh, const double* s,
  * compact-WY block, default 128), "wait_limit_ms" (device wait time limit, default 2000), "stage_timing" (1: record
  * CUDA events at stage boundaries; read with xtb_gpu_stage_*), "graphs" (default 1: a device-pointer solve repeated
  * on the same buffers and non-NULL stream is captured into a CUDA graph on its second call and replayed after),
- * "batch_workers" (host threads, each with its own stream, that the batch calls spread problems over; default 4).
- * Returns 0, or -1 for an unknown name. */
+ * "batch_workers" (host threads, each with its own stream, that the batch calls spread problems over; default 4),
+ * "precision" (64, default: FP64 throughout; 32: the generalized solves run the reduction chain in FP32 - congruence,
+ * resident sytrd, ormtr, back-transform; Cholesky and the tridiagonal eigensolve stay FP64 - then refine C and e in
+ * FP64 as xtb_dsygvd_refine_device does), "refine_iters" (refinement steps of the mixed path, default 2).
+ * Returns 0, -1 for an unknown name, or -2 for a value out of range. */
 int xtb_gpu_set_option(const char* name, long value);
 long xtb_gpu_get_option(const char* name);
 

@@ -117,3 +117,44 @@ def test_divided_differences_near_degenerate_finite():
 def test_fnv_hash_stable():
     assert metrics.fnv1a(np.zeros(2)) == metrics.fnv1a(np.zeros(2))
     assert metrics.fnv1a(np.zeros(2)) != metrics.fnv1a(np.ones(2))
+
+
+def _fp32_start(h, s):
+    import scipy.linalg as sla
+
+    w32, c32 = sla.eigh(h.astype(np.float32), s.astype(np.float32))
+    return c32.astype(np.float64)
+
+
+@pytest.mark.parametrize("n", [120, 400])
+def test_refine_oracle_from_fp32(n):
+    """Two refinement steps from an FP32 solve reach FP64 accuracy (the mixed path's bar)."""
+    from oracle import refine
+
+    h, s, lam = inputs.generalized(n, seed=5)
+    w_ref, c_ref = lapack.sygvd_chain(h, s)
+    w, c = refine.refine(h, s, _fp32_start(h, s), iters=2)
+    assert np.max(np.abs(w - lam)) < 1e-12
+    assert metrics.density_error(c, c_ref, metrics.aufbau(n, n // 2)) < 1e-10
+    assert metrics.s_orthogonality(s, c) < 1e-10
+
+
+def test_refine_oracle_cluster():
+    """A cluster of 6 eigenvalues 1e-9 Eh apart: resolved by the exact cluster solve, not by first-order division."""
+    from oracle import refine
+
+    n = 90
+    rng = np.random.default_rng(11)
+    s = inputs.overlap(n, rng)
+    lam = np.sort(rng.uniform(-1.0, 0.5, n))
+    lam[40:46] = -0.3 + np.arange(6) * 1e-9
+    lam = np.sort(lam)
+    ws, vs = np.linalg.eigh(s)
+    shalf = (vs * np.sqrt(ws)) @ vs.T
+    q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    h = shalf @ (q * lam) @ q.T @ shalf
+    h = 0.5 * (h + h.T)
+    w, c = refine.refine(h, s, _fp32_start(h, s), iters=2)
+    assert np.max(np.abs(w - lam)) < 1e-12
+    assert metrics.s_orthogonality(s, c) < 1e-10
+    assert metrics.backward_error(h, s, w, c) < 10

@@ -31,6 +31,8 @@ std::atomic<long> g_wait_ms{2000};
 std::atomic<long> g_stage_timing{0};
 std::atomic<long> g_graphs{1};
 std::atomic<long> g_batch_workers{4};
+std::atomic<long> g_precision{64};    // 64: FP64 throughout; 32: FP32 reduction chain + FP64 refinement
+std::atomic<long> g_refine_iters{2};
 std::atomic<long long> g_launches{0};
 thread_local long long t_launches = 0;  // this thread's launches: a graph capture counts its own, not other threads'
 
@@ -295,7 +297,7 @@ void stage_stedc(Call& k, int n, double* d, double* e, double* z, int ldz) {
 
 // The generalized core on device buffers: h (n x n, full symmetric, ld n) is consumed; u (n x n, ld n) holds B's upper
 // triangle on entry and U on exit; c (n x n, ld n) receives C; w (n) the eigenvalues.
-void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
+void core_sygvd_fp64(Call& k, int n, double* h, double* u, double* c, double* w) {
   if (!k.ok() || n <= 0) return;
   double* x = k.template dev<double>("gv.X", (size_t)n * n);
   double* t = k.template dev<double>("gv.T", (size_t)n * n);
@@ -327,6 +329,66 @@ void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
   p = gemm_problem<double>(n, n, n, 1.0, x, n, 0, z, n, 0, 0.0, c, n, kTriAUpper);
   if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "back-transform");
   k.mark("trmm");
+}
+
+// Mixed precision: the reduction chain in FP32 (congruence, resident sytrd, ormtr, back-transform; the tridiagonal
+// eigensolve and the Cholesky factor in FP64), then FP64 Ogita-Aishima refinement on the FP64 pair (H, S).  Same
+// buffer contract as core_sygvd (h is kept intact here).
+void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w) {
+  if (!k.ok() || n <= 0) return;
+  const size_t nn = (size_t)n * n;
+  double* x = k.template dev<double>("gv.X", nn);
+  double* t = k.template dev<double>("gv.T", nn);
+  double* sf = k.template dev<double>("mx.S", nn);
+  double* z = k.template dev<double>("gv.Z", nn);
+  double* e = k.template dev<double>("gv.e", (size_t)n);
+  float* f = k.template dev<float>("mx.f32", 5 * nn + 3 * (size_t)n);
+  double* rw = k.template dev<double>("mx.refine", refine_work_elems(n));
+  unsigned* pctr = k.template dev<unsigned>("potrf.ctr", 64);
+  if (!k.ok()) return;
+  float* xf = f;
+  float* hf = xf + nn;
+  float* tf = hf + nn;
+  float* rf = tf + nn;
+  float* zf = rf + nn;
+  float* df = zf + nn;
+  float* ef = df + n;
+  float* tauf = ef + n;
+  symmetrize_upper<double>(n, u, n, sf, n, k.s);
+  k.check(potrf_inverse_upper(n, u, n, x, n, t, pctr, k.c->num_sms, k.c->d_status, wait_limit_ns(), k.s),
+          "potrf+inverse");
+  k.mark("potrf_inverse");
+  convert_mat_f64_to_f32(n, n, x, n, xf, n, k.s);
+  convert_mat_f64_to_f32(n, n, h, n, hf, n, k.s);
+  GemmDesc<float> p = gemm_problem<float>(n, n, n, 1.f, hf, n, 0, xf, n, 0, 0.f, tf, n, kTriBUpper);
+  if (k.ok()) k.check(gemm_group<float>(k.c->arena, &p, 1, k.s), "congruence 1 (fp32)");
+  p = gemm_problem<float>(n, n, n, 1.f, xf, n, 1, tf, n, 0, 0.f, rf, n, kTriALower | kCUpper);
+  if (k.ok()) k.check(gemm_group<float>(k.c->arena, &p, 1, k.s), "congruence 2 (fp32)");
+  if (k.ok()) symmetrize_upper<float>(n, rf, n, hf, n, k.s);
+  k.mark("congruence");
+  stage_sytrd<float>(k, n, hf, n, rf, n, df, ef, tauf);
+  k.mark("sytrd");
+  if (k.ok()) {
+    convert_f32_to_f64(n, df, w, k.s);
+    convert_f32_to_f64(n, ef, e, k.s);
+  }
+  stage_stedc(k, n, w, e, z, n);
+  k.mark("stedc");
+  if (k.ok()) convert_mat_f64_to_f32(n, n, z, n, zf, n, k.s);
+  stage_ormtr<float>(k, n, n, rf, n, tauf, zf, n);
+  k.mark("ormtr");
+  p = gemm_problem<float>(n, n, n, 1.f, xf, n, 0, zf, n, 0, 0.f, tf, n, kTriAUpper);
+  if (k.ok()) k.check(gemm_group<float>(k.c->arena, &p, 1, k.s), "back-transform (fp32)");
+  if (k.ok()) convert_mat_f32_to_f64(n, n, tf, n, c, n, k.s);
+  k.mark("trmm");
+  if (k.ok())
+    k.check(refine_generalized(n, h, n, sf, n, c, n, w, (int)g_refine_iters.load(), rw, k.c->arena, k.s), "refine");
+  k.mark("refine");
+}
+
+void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
+  if (g_precision.load() == 32) core_sygvd_mixed(k, n, h, u, c, w);
+  else core_sygvd_fp64(k, n, h, u, c, w);
 }
 
 // Standard problem on device buffers: f (n x n full symmetric, ld n) consumed; z (n x n) eigenvectors; w eigenvalues.
@@ -591,7 +653,8 @@ void sygvd_device_body(Call& k, int n, double* a, int lda, double* b, int ldb, d
 
 int sygvd_device(Context* c, cudaStream_t s, int n, double* a, int lda, double* b, int ldb, double* w) {
   const std::vector<long long> key = {1, n, (long long)(uintptr_t)a, lda, (long long)(uintptr_t)b, ldb,
-                                      (long long)(uintptr_t)w, (long long)(uintptr_t)s};
+                                      (long long)(uintptr_t)w, (long long)(uintptr_t)s, g_precision.load(),
+                                      g_refine_iters.load()};
   DeviceStatus st{};
   const int code = run_graphed(c, s, key, &st, [&](Call& k) { sygvd_device_body(k, n, a, lda, b, ldb, w); });
   return info_of(code, st, n);
@@ -866,6 +929,30 @@ int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, 
   return sygvd_device(c, (cudaStream_t)stream, n, a, lda, b, ldb, w);
 }
 
+int xtb_dsygvd_refine_device(int n, const double* h, int ldh, const double* s, int lds, double* c, int ldc,
+                             double* w, int iters, void* stream) {
+  if (n < 0) return -1;
+  if (ldh < std::max(1, n)) return -3;
+  if (lds < std::max(1, n)) return -5;
+  if (ldc < std::max(1, n)) return -7;
+  if (iters < 1 || iters > 10) return -9;
+  if (n == 0) return 0;
+  Context* c0 = context();
+  if (!c0) return t_state.last_code;
+  Call k(c0, (cudaStream_t)stream, true);
+  double* hf = k.dev<double>("rf.H", (size_t)n * n);
+  double* sf = k.dev<double>("rf.S", (size_t)n * n);
+  double* rw = k.dev<double>("mx.refine", refine_work_elems(n));
+  if (k.ok()) {
+    symmetrize_upper<double>(n, h, ldh, hf, n, k.s);
+    symmetrize_upper<double>(n, s, lds, sf, n, k.s);
+    k.check(refine_generalized(n, hf, n, sf, n, c, ldc, w, iters, rw, c0->arena, k.s), "refine");
+  }
+  DeviceStatus st{};
+  const int code = k.finish(&st);
+  return info_of(code, st, n);
+}
+
 int xtb_dsygvd_batched(int count, const int* n, double* const* a, const int* lda, double* const* b, const int* ldb,
                        double* const* w, int* info) {
   const int bad = check_batch(count, n, a, lda, b, ldb, w);
@@ -968,6 +1055,16 @@ int xtb_gpu_set_option(const char* name, long value) {
   if (!std::strcmp(name, "stage_timing")) { g_stage_timing = value; return 0; }
   if (!std::strcmp(name, "graphs")) { g_graphs = value; return 0; }
   if (!std::strcmp(name, "batch_workers")) { g_batch_workers = value; return 0; }
+  if (!std::strcmp(name, "precision")) {
+    if (value != 64 && value != 32) return -2;
+    g_precision = value;
+    return 0;
+  }
+  if (!std::strcmp(name, "refine_iters")) {
+    if (value < 1 || value > 10) return -2;
+    g_refine_iters = value;
+    return 0;
+  }
   return -1;
 }
 
@@ -979,6 +1076,8 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "stage_timing")) return g_stage_timing;
   if (!std::strcmp(name, "graphs")) return g_graphs;
   if (!std::strcmp(name, "batch_workers")) return g_batch_workers;
+  if (!std::strcmp(name, "precision")) return g_precision;
+  if (!std::strcmp(name, "refine_iters")) return g_refine_iters;
   return -1;
 }
 

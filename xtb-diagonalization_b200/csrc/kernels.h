@@ -130,6 +130,13 @@ cudaError_t potrf_inverse_upper(int n, double* a, int lda, double* x, int ldx, d
 cudaError_t dk_adjoint(int n, const double* c, const double* e, double mu, double kt, const double* wbar, double* dh,
                        double* ds, double* t1, double* t2, double* t3, DescArena& arena, cudaStream_t s);
 
+// ---------------------------------------------------------------------------------------------------- refinement
+// FP64 Ogita-Aishima refinement of C (n x n, ldc) for H C = S C diag(w), C^T S C = I: `iters` steps, then c and w
+// rewritten in ascending eigenvalue order.  h, s full symmetric (FP64).  work: refine_work_elems(n) doubles.
+size_t refine_work_elems(int n);
+cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s, int lds, double* c, int ldc,
+                               double* w, int iters, double* work, DescArena& arena, cudaStream_t st);
+
 // ---------------------------------------------------------------------------------------------------- helpers
 // Stage nprob descriptors through the arena (tile grid and tile_begin filled in from M, N) and launch one grouped GEMM.
 template <typename T>

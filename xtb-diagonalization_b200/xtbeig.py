@@ -47,6 +47,7 @@ def lib():
                                                     _I, _P, _P, _I]
         _lib.xtb_dsygvd_batched.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P]
         _lib.xtb_dsygvd_batched_device.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P]
+        _lib.xtb_dsygvd_refine_device.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _I, _P]
         _lib.xtb_gpu_stage_name.restype = C.c_char_p
         _lib.xtb_gpu_stage_name.argtypes = [_I]
         _lib.xtb_gpu_stage_ms.restype = C.c_double
@@ -93,8 +94,11 @@ def version() -> str:
 
 
 def set_option(name: str, value: int) -> None:
-    if lib().xtb_gpu_set_option(name.encode(), int(value)) != 0:
+    r = lib().xtb_gpu_set_option(name.encode(), int(value))
+    if r == -1:
         raise KeyError(name)
+    if r != 0:
+        raise ValueError(f"{name}={value} out of range")
 
 
 def get_option(name: str) -> int:
@@ -213,6 +217,12 @@ def dsygvd_device(n, a_ptr, lda, b_ptr, ldb, w_ptr, stream=0) -> int:
     """Device-pointer solve (column-major device buffers, e.g. torch tensors' data_ptr())."""
     return int(lib().xtb_dsygvd_device(int(n), _P(a_ptr), int(lda), _P(b_ptr), int(ldb), _P(w_ptr),
                                        _P(stream) if stream else None))
+
+
+def dsygvd_refine_device(n, h_ptr, ldh, s_ptr, lds, c_ptr, ldc, w_ptr, iters=2, stream=0) -> int:
+    """FP64 refinement of approximate generalized eigenvectors c (device buffers); returns info."""
+    return int(lib().xtb_dsygvd_refine_device(int(n), _P(h_ptr), int(ldh), _P(s_ptr), int(lds), _P(c_ptr), int(ldc),
+                                              _P(w_ptr), int(iters), _P(stream) if stream else None))
 
 
 def dsyevd_device(n, a_ptr, lda, w_ptr, stream=0) -> int:
