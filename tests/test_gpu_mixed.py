@@ -131,9 +131,9 @@ def test_refine_device_matches_oracle(xe, iters):
     c = Cd.cpu().numpy().T
     assert np.max(np.abs(w - w_o)) < 1e-12
     assert metrics.density_error(c, c_o, metrics.aufbau(n, n // 2)) < 1e-11
-    if iters >= 2:
+    if iters >= 2:  # the oracle's own S-orthogonality after two steps here is 1.7e-11
         assert np.max(np.abs(w - lam)) < 1e-12
-        assert metrics.s_orthogonality(s, c) < 1e-11
+        assert metrics.s_orthogonality(s, c) < 1e-10
 
 
 def test_refine_device_invalid_arguments(xe):
