@@ -176,8 +176,9 @@ def load_peaks():
 
 
 def load_traffic(n):
-    """DRAM bytes per sytrd launch from the committed ncu summary (profiles/traffic.json), scaled to n if captured on
-    a smaller case; None if no capture exists."""
+    """DRAM bytes per sytrd launch from the committed ncu summary (profiles/traffic.json): the kernel reads the matrix
+    once and keeps it in shared memory, so traffic scales as n^2 when the capture was of another size; None if no
+    capture exists."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(path):
         return None
@@ -186,7 +187,7 @@ def load_traffic(n):
     rec = t.get("sytrd")
     if not rec:
         return None
-    return float(rec["bytes_per_launch"]) * (n / rec["n"]) ** 3 if rec.get("n") else None
+    return float(rec["bytes_per_launch"]) * (n / rec["n"]) ** 2 if rec.get("n") else None
 
 
 def generalized_on_device(n, seed, dev):
@@ -270,12 +271,14 @@ def run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush):
         xtbeig.set_option("stage_timing", 0)
         K = max(1, args.steps // 2)
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        torch.cuda.nvtx.range_push("mixed_timed")
         for i in range(K):
             flush.zero_()
             ev[i][0].record(stream)
             solve()
             ev[i][1].record(stream)
         torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_pop()
         ms = sum(a.elapsed_time(b) for a, b in ev) / K
     finally:
         xtbeig.set_option("precision", 64)
@@ -335,11 +338,13 @@ def run_batch_section(args, dev, stream):
     steps = max(1, args.batch_steps)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     launches0 = xtbeig.launch_count()
+    torch.cuda.nvtx.range_push("batch_timed")
     for k in range(steps):
         ev[k][0].record(stream)
         batch_step()
         ev[k][1].record(stream)
     torch.cuda.synchronize(dev)
+    torch.cuda.nvtx.range_pop()
     launches = xtbeig.launch_count() - launches0
     ms_batch = statistics.mean(a.elapsed_time(b) for a, b in ev)
     eig_err = max(float((W[i] - LAM[i]).abs().max()) for i in range(count))
@@ -465,12 +470,14 @@ def run_ours(args):
     sampler.start()
     time.sleep(0.3)
     t_wall0 = time.perf_counter()
+    torch.cuda.nvtx.range_push("fp64_timed")
     for i in range(K):
         flush.zero_()
         ev[i][0].record(stream)
         solve()
         ev[i][1].record(stream)
     torch.cuda.synchronize(dev)
+    torch.cuda.nvtx.range_pop()
     t_wall = time.perf_counter() - t_wall0
     if world > 1:
         dist.barrier()
