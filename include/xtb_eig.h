@@ -96,6 +96,15 @@ int xtb_dsytrd_upper_noalloc(int n, double* a, int lda, double* d, double* e, do
 int xtb_dsygvd_refine_device(int n, const double* h, int ldh, const double* s, int lds, double* c, int ldc,
                              double* w, int iters, void* stream);
 
+/* FP32 GEMM on the tcgen05 tensor cores, DEVICE pointers, column-major as BLAS sgemm:
+ * C = alpha op(A) op(B) + beta C, op(X) = X (trans 0) or X^T (trans 1), op(A) m x k, op(B) k x n.  passes = 3 splits
+ * every operand into two TF32 parts and keeps three products (about FP32 accuracy); passes = 1 is plain TF32.  This
+ * is the engine of the mixed solve's FP32 GEMMs (the reference runs them as Accelerate sgemm calls inside its FP32
+ * eigensolver, e.g. Sources/Diagonalization/TridiagonalBackTransformation.swift:18-45).  Queued on `stream` and
+ * synchronised.  Returns 0, -(argument position) for an invalid argument, -1000 - cudaError, or a device status code. */
+int xtb_sgemm_tc_device(int transa, int transb, int m, int n, int k, float alpha, const float* a, int lda,
+                        const float* b, int ldb, float beta, float* c, int ldc, int passes, void* stream);
+
 /* A batch of independent generalized problems (host arrays, itype 1, jobz 'V', uplo 'U'): problem i has size n[i],
  * a[i] (lda[i]), b[i] (ldb[i]), w[i]; info[i] per problem (info may be NULL).  The problems are assigned to the
  * library's worker threads longest first (static LPT on a cost model of n), each worker with its own stream and
@@ -127,7 +136,9 @@ int xtb_dsygvd_density_adjoint(int n, const double* h, int ldh, const double* s,
  * "batch_workers" (host threads, each with its own stream, that the batch calls spread problems over; default 4),
  * "precision" (64, default: FP64 throughout; 32: the generalized solves run the reduction chain in FP32 - congruence,
  * resident sytrd, ormtr, back-transform; Cholesky and the tridiagonal eigensolve stay FP64 - then refine C and e in
- * FP64 as xtb_dsygvd_refine_device does), "refine_iters" (refinement steps of the mixed path, default 2).
+ * FP64 as xtb_dsygvd_refine_device does), "refine_iters" (refinement steps of the mixed path, default 2),
+ * "mixed_gemm" (engine of the mixed path's FP32 GEMMs: 3 = 3xTF32 on the tcgen05 tensor cores, default; 1 = TF32;
+ * 0 = FP32 on the CUDA cores).
  * Returns 0, -1 for an unknown name, or -2 for a value out of range. */
 int xtb_gpu_set_option(const char* name, long value);
 long xtb_gpu_get_option(const char* name);

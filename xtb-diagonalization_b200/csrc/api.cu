@@ -33,6 +33,7 @@ std::atomic<long> g_graphs{1};
 std::atomic<long> g_batch_workers{4};
 std::atomic<long> g_precision{64};    // 64: FP64 throughout; 32: FP32 reduction chain + FP64 refinement
 std::atomic<long> g_refine_iters{2};
+std::atomic<long> g_mixed_gemm{3};    // FP32 GEMMs of the mixed solve: 0 CUDA cores, 1 TF32, 3 3xTF32 (tcgen05)
 std::atomic<long long> g_launches{0};
 thread_local long long t_launches = 0;  // this thread's launches: a graph capture counts its own, not other threads'
 
@@ -270,12 +271,24 @@ void stage_sytrd(Call& k, int n, const T* dfull, int ldf, T* dout, int lda, T* d
 }
 
 template <typename T>
-void stage_ormtr(Call& k, int n, int m, const T* a, int lda, const T* tau, T* z, int ldz) {
+void stage_ormtr(Call& k, int n, int m, const T* a, int lda, const T* tau, T* z, int ldz, const TcGemm& tc = TcGemm()) {
   if (!k.ok() || n <= 1 || m <= 0) return;
   const int nb = (int)std::max<long>(16, g_ormtr_nb.load());
   T* w = k.template dev<T>("ormtr.work", ormtr_work_elems<T>(n, m, nb));
   if (!k.ok()) return;
-  k.check(ormtr_upper<T>(n, m, a, lda, tau, z, ldz, nb, ormtr_carve<T>(w, n, m, nb), k.c->arena, k.s), "ormtr");
+  k.check(ormtr_upper<T>(n, m, a, lda, tau, z, ldz, nb, ormtr_carve<T>(w, n, m, nb), k.c->arena, k.s, tc), "ormtr");
+}
+
+// The tcgen05 engine for the FP32 GEMMs of an n x n mixed solve (passes from the mixed_gemm option; 0 = CUDA cores).
+TcGemm tc_engine(Call& k, int n) {
+  TcGemm tc;
+  tc.passes = (int)g_mixed_gemm.load();
+  if (tc.passes == 0) return tc;
+  tc.work_elems = tc_work_elems(n);
+  tc.work = k.template dev<float>("tc.work", tc.work_elems);
+  tc.st = k.c->d_status;
+  tc.limit_ns = wait_limit_ns();
+  return tc;
 }
 
 void stage_stedc(Call& k, int n, double* d, double* e, double* z, int ldz) {
@@ -354,6 +367,8 @@ void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w
   float* df = zf + nn;
   float* ef = df + n;
   float* tauf = ef + n;
+  const TcGemm tc = tc_engine(k, n);
+  if (!k.ok()) return;
   symmetrize_upper<double>(n, u, n, sf, n, k.s);
   k.check(potrf_inverse_upper(n, u, n, x, n, t, pctr, k.c->num_sms, k.c->d_status, wait_limit_ns(), k.s),
           "potrf+inverse");
@@ -361,9 +376,9 @@ void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w
   convert_mat_f64_to_f32(n, n, x, n, xf, n, k.s);
   convert_mat_f64_to_f32(n, n, h, n, hf, n, k.s);
   GemmDesc<float> p = gemm_problem<float>(n, n, n, 1.f, hf, n, 0, xf, n, 0, 0.f, tf, n, kTriBUpper);
-  if (k.ok()) k.check(gemm_group<float>(k.c->arena, &p, 1, k.s), "congruence 1 (fp32)");
+  if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "congruence 1 (fp32)");
   p = gemm_problem<float>(n, n, n, 1.f, xf, n, 1, tf, n, 0, 0.f, rf, n, kTriALower | kCUpper);
-  if (k.ok()) k.check(gemm_group<float>(k.c->arena, &p, 1, k.s), "congruence 2 (fp32)");
+  if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "congruence 2 (fp32)");
   if (k.ok()) symmetrize_upper<float>(n, rf, n, hf, n, k.s);
   k.mark("congruence");
   stage_sytrd<float>(k, n, hf, n, rf, n, df, ef, tauf);
@@ -375,10 +390,10 @@ void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w
   stage_stedc(k, n, w, e, z, n);
   k.mark("stedc");
   if (k.ok()) convert_mat_f64_to_f32(n, n, z, n, zf, n, k.s);
-  stage_ormtr<float>(k, n, n, rf, n, tauf, zf, n);
+  stage_ormtr<float>(k, n, n, rf, n, tauf, zf, n, tc);
   k.mark("ormtr");
   p = gemm_problem<float>(n, n, n, 1.f, xf, n, 0, zf, n, 0, 0.f, tf, n, kTriAUpper);
-  if (k.ok()) k.check(gemm_group<float>(k.c->arena, &p, 1, k.s), "back-transform (fp32)");
+  if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "back-transform (fp32)");
   if (k.ok()) convert_mat_f32_to_f64(n, n, tf, n, c, n, k.s);
   k.mark("trmm");
   if (k.ok())
@@ -953,6 +968,29 @@ int xtb_dsygvd_refine_device(int n, const double* h, int ldh, const double* s, i
   return info_of(code, st, n);
 }
 
+int xtb_sgemm_tc_device(int transa, int transb, int m, int n, int k_, float alpha, const float* a, int lda,
+                        const float* b, int ldb, float beta, float* c, int ldc, int passes, void* stream) {
+  if (transa != 0 && transa != 1) return -1;
+  if (transb != 0 && transb != 1) return -2;
+  if (m < 0) return -3;
+  if (n < 0) return -4;
+  if (k_ < 0) return -5;
+  if (lda < std::max(1, transa ? k_ : m)) return -8;
+  if (ldb < std::max(1, transb ? n : k_)) return -10;
+  if (ldc < std::max(1, m)) return -13;
+  if (passes != 1 && passes != 3) return -14;
+  if (m == 0 || n == 0) return 0;
+  Context* c0 = context();
+  if (!c0) return t_state.last_code;
+  Call k(c0, (cudaStream_t)stream, true);
+  GemmDesc<float> p = gemm_problem<float>(m, n, k_, alpha, a, lda, transa, b, ldb, transb, beta, c, ldc);
+  const size_t we = umma_work_elems(&p, 1);
+  float* w = k.dev<float>("tc.work", we);
+  if (k.ok()) k.check(umma_gemm_group(&p, 1, passes, w, we, c0->d_status, wait_limit_ns(), k.s), "tcgen05 sgemm");
+  DeviceStatus st{};
+  return k.finish(&st);
+}
+
 int xtb_dsygvd_batched(int count, const int* n, double* const* a, const int* lda, double* const* b, const int* ldb,
                        double* const* w, int* info) {
   const int bad = check_batch(count, n, a, lda, b, ldb, w);
@@ -1065,6 +1103,11 @@ int xtb_gpu_set_option(const char* name, long value) {
     g_refine_iters = value;
     return 0;
   }
+  if (!std::strcmp(name, "mixed_gemm")) {
+    if (value != 0 && value != 1 && value != 3) return -2;
+    g_mixed_gemm = value;
+    return 0;
+  }
   return -1;
 }
 
@@ -1078,6 +1121,7 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "batch_workers")) return g_batch_workers;
   if (!std::strcmp(name, "precision")) return g_precision;
   if (!std::strcmp(name, "refine_iters")) return g_refine_iters;
+  if (!std::strcmp(name, "mixed_gemm")) return g_mixed_gemm;
   return -1;
 }
 

@@ -125,6 +125,15 @@ cudaError_t gemm_group(DescArena& arena, const GemmDesc<T>* probs, int nprob, cu
   return cudaGetLastError();
 }
 
+cudaError_t gemm_run(DescArena& arena, const TcGemm&, const GemmDesc<double>* probs, int nprob, cudaStream_t s) {
+  return gemm_group<double>(arena, probs, nprob, s);
+}
+
+cudaError_t gemm_run(DescArena& arena, const TcGemm& tc, const GemmDesc<float>* probs, int nprob, cudaStream_t s) {
+  if (tc.passes == 0) return gemm_group<float>(arena, probs, nprob, s);
+  return umma_gemm_group(probs, nprob, tc.passes, tc.work, tc.work_elems, tc.st, tc.limit_ns, s);
+}
+
 template GemmDesc<double> gemm_problem<double>(int, int, int, double, const double*, int, int, const double*, int,
                                                int, double, double*, int, int);
 template GemmDesc<float> gemm_problem<float>(int, int, int, float, const float*, int, int, const float*, int, int,

@@ -72,6 +72,28 @@ void convert_f64_to_f32(size_t count, const double* src, float* dst, cudaStream_
 void convert_mat_f32_to_f64(int m, int n, const float* a, int lda, double* b, int ldb, cudaStream_t s);
 void convert_mat_f64_to_f32(int m, int n, const double* a, int lda, float* b, int ldb, cudaStream_t s);
 
+// ---------------------------------------------------------------------------------------------------- GEMM engines
+// tcgen05 TF32 GEMMs for FP32 problems (umma_gemm.cu): passes 1 = TF32, 3 = 3xTF32 (about FP32 accuracy).  `work`
+// holds the split operands (umma_work_elems floats for the group); sizes beyond it are refused.
+size_t umma_work_elems(const GemmDesc<float>* probs, int nprob);
+cudaError_t umma_gemm_group(const GemmDesc<float>* probs, int nprob, int passes, float* work, size_t work_elems,
+                            DeviceStatus* st, uint64_t limit_ns, cudaStream_t s);
+// Floats of tcgen05 GEMM workspace that every GEMM of an n x n solve stage fits in.
+inline size_t tc_work_elems(int n) { return 6 * (size_t)(n + 64) * (size_t)(n + 64); }
+
+struct DescArena;
+// Which engine runs a stage's GEMMs: passes 0 = the grouped GEMM (FP64 DMMA / FP32 CUDA cores); for FP32 problems
+// passes 1 or 3 = the tcgen05 engine.
+struct TcGemm {
+  int passes = 0;
+  float* work = nullptr;
+  size_t work_elems = 0;
+  DeviceStatus* st = nullptr;
+  uint64_t limit_ns = 0;
+};
+cudaError_t gemm_run(DescArena& arena, const TcGemm& tc, const GemmDesc<double>* probs, int nprob, cudaStream_t s);
+cudaError_t gemm_run(DescArena& arena, const TcGemm& tc, const GemmDesc<float>* probs, int nprob, cudaStream_t s);
+
 // ---------------------------------------------------------------------------------------------------- ormtr
 // Z(0:n, 0:m) <- Q Z with Q = H(n-2) ... H(0) from sytrd (upper).  Workspace layout in OrmtrWork.
 // Descriptor arena: GEMM descriptors are staged in pinned host memory and copied to device memory on the stream.
@@ -105,7 +127,7 @@ template <typename T>
 OrmtrWork<T> ormtr_carve(T* base, int n, int m, int nb);
 template <typename T>
 cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, int ldz, int nb, OrmtrWork<T> w,
-                        DescArena& arena, cudaStream_t s);
+                        DescArena& arena, cudaStream_t s, const TcGemm& tc = TcGemm());
 
 // ---------------------------------------------------------------------------------------------------- stedc
 struct StedcWork;  // opaque, sized by stedc_work_bytes

@@ -60,7 +60,7 @@ OrmtrWork<T> ormtr_carve(T* base, int n, int m, int nb) {
 
 template <typename T>
 cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, int ldz, int nb, OrmtrWork<T> w,
-                        DescArena& arena, cudaStream_t s) {
+                        DescArena& arena, cudaStream_t s, const TcGemm& tc) {
   if (n <= 1 || m <= 0) return cudaSuccess;
   const int nm1 = n - 1;
   const int nblocks = (nm1 + nb - 1) / nb;
@@ -76,7 +76,7 @@ cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, i
     const T* vb = w.V + (size_t)j0 * n;
     probs[b] = gemm_problem<T>(kb, kb, rows, T(1), vb, n, 1, vb, n, 0, T(0), w.Tf + (size_t)b * nb * nb, nb);
   }
-  cudaError_t err = gemm_group<T>(arena, probs, nblocks, s);
+  cudaError_t err = gemm_run(arena, tc, probs, nblocks, s);
   if (err != cudaSuccess) { delete[] probs; return err; }
   {
     const size_t smem = ((size_t)nb * nb + nb) * sizeof(T);
@@ -90,7 +90,7 @@ cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, i
     probs[b] = gemm_problem<T>(rows, kb, kb, T(1), w.V + (size_t)j0 * n, n, 0, w.Tf + (size_t)b * nb * nb, nb, 1,
                                T(0), w.Y + (size_t)j0 * n, n, kTriBLower);
   }
-  err = gemm_group<T>(arena, probs, nblocks, s);
+  err = gemm_run(arena, tc, probs, nblocks, s);
   delete[] probs;
   if (err != cudaSuccess) return err;
   // Apply the blocks in increasing order.  W = V_b^T Z has only kb (<= nb) rows, so its long K (the block's rows) is
@@ -98,10 +98,10 @@ cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, i
   T* parts = w.W + (size_t)nb * m;
   for (int b = 0; b < nblocks; ++b) {
     const int j0 = b * nb, kb = std::min(nb, nm1 - j0), rows = j0 + kb;
-    const int S = split_count(kb, m, rows);
+    const int S = tc.passes ? split_count(kb, m, rows, 128, 128) : split_count(kb, m, rows);
     if (S == 1) {
       GemmDesc<T> p1 = gemm_problem<T>(kb, m, rows, T(1), w.V + (size_t)j0 * n, n, 1, z, ldz, 0, T(0), w.W, nb);
-      err = gemm_group<T>(arena, &p1, 1, s);
+      err = gemm_run(arena, tc, &p1, 1, s);
     } else {
       GemmDesc<T> ps[kMaxSplit];
       const int ks = ((rows + S - 1) / S + kGemmBK - 1) / kGemmBK * kGemmBK;
@@ -112,7 +112,7 @@ cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, i
         ps[used++] = gemm_problem<T>(kb, m, kr, T(1), w.V + r0 + (size_t)j0 * n, n, 1, z + r0, ldz, 0, T(0),
                                      parts + (size_t)sl * nb * m, nb);
       }
-      err = gemm_group<T>(arena, ps, used, s);
+      err = gemm_run(arena, tc, ps, used, s);
       if (err == cudaSuccess) {
         const size_t total = (size_t)kb * m;
         const int grid = (int)std::min<size_t>((total + 255) / 256, 148 * 8);
@@ -121,7 +121,7 @@ cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, i
     }
     if (err != cudaSuccess) return err;
     GemmDesc<T> p2 = gemm_problem<T>(rows, m, kb, T(-1), w.Y + (size_t)j0 * n, n, 0, w.W, nb, 0, T(1), z, ldz);
-    err = gemm_group<T>(arena, &p2, 1, s);
+    err = gemm_run(arena, tc, &p2, 1, s);
     if (err != cudaSuccess) return err;
   }
   return cudaGetLastError();
@@ -132,8 +132,8 @@ template size_t ormtr_work_elems<float>(int, int, int);
 template OrmtrWork<double> ormtr_carve<double>(double*, int, int, int);
 template OrmtrWork<float> ormtr_carve<float>(float*, int, int, int);
 template cudaError_t ormtr_upper<double>(int, int, const double*, int, const double*, double*, int, int,
-                                         OrmtrWork<double>, DescArena&, cudaStream_t);
+                                         OrmtrWork<double>, DescArena&, cudaStream_t, const TcGemm&);
 template cudaError_t ormtr_upper<float>(int, int, const float*, int, const float*, float*, int, int,
-                                        OrmtrWork<float>, DescArena&, cudaStream_t);
+                                        OrmtrWork<float>, DescArena&, cudaStream_t, const TcGemm&);
 
 }  // namespace xtbeig

@@ -59,8 +59,8 @@ __global__ void splitk_sum_kernel(int kb, int m, int nb, int S, const T* __restr
 constexpr int kMaxSplit = 8;
 
 // Split-K slices for W = V_b^T Z: enough CTAs to cover the SMs twice, slices of at least 128 rows.
-inline int split_count(int kb, int m, int rows) {
-  const int tiles = ((kb + kGemmBM - 1) / kGemmBM) * ((m + kGemmBN - 1) / kGemmBN);
+inline int split_count(int kb, int m, int rows, int bm = kGemmBM, int bn = kGemmBN) {
+  const int tiles = ((kb + bm - 1) / bm) * ((m + bn - 1) / bn);
   int S = (2 * 148 + tiles - 1) / tiles;
   S = std::min(S, std::max(1, rows / 128));
   return std::max(1, std::min(S, kMaxSplit));

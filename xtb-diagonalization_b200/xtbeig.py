@@ -48,6 +48,8 @@ def lib():
         _lib.xtb_dsygvd_batched.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P]
         _lib.xtb_dsygvd_batched_device.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P]
         _lib.xtb_dsygvd_refine_device.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _I, _P]
+        _lib.xtb_sgemm_tc_device.argtypes = [_I, _I, _I, _I, _I, C.c_float, _P, _I, _P, _I, C.c_float, _P, _I, _I,
+                                             _P]
         _lib.xtb_gpu_stage_name.restype = C.c_char_p
         _lib.xtb_gpu_stage_name.argtypes = [_I]
         _lib.xtb_gpu_stage_ms.restype = C.c_double
@@ -223,6 +225,13 @@ def dsygvd_refine_device(n, h_ptr, ldh, s_ptr, lds, c_ptr, ldc, w_ptr, iters=2, 
     """FP64 refinement of approximate generalized eigenvectors c (device buffers); returns info."""
     return int(lib().xtb_dsygvd_refine_device(int(n), _P(h_ptr), int(ldh), _P(s_ptr), int(lds), _P(c_ptr), int(ldc),
                                               _P(w_ptr), int(iters), _P(stream) if stream else None))
+
+
+def sgemm_tc_device(transa, transb, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc, passes=3,
+                    stream=0) -> int:
+    """xtb_sgemm_tc_device: FP32 GEMM on the tcgen05 tensor cores (3xTF32 or TF32) on device pointers."""
+    return lib().xtb_sgemm_tc_device(transa, transb, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc, passes,
+                                     stream)
 
 
 def dsyevd_device(n, a_ptr, lda, w_ptr, stream=0) -> int:
