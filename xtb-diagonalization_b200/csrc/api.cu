@@ -33,7 +33,9 @@ std::atomic<long> g_graphs{1};
 std::atomic<long> g_batch_workers{4};
 std::atomic<long> g_precision{64};    // 64: FP64 throughout; 32: FP32 reduction chain + FP64 refinement
 std::atomic<long> g_refine_iters{2};
-std::atomic<long> g_mixed_gemm{3};    // FP32 GEMMs of the mixed solve: 0 CUDA cores, 1 TF32, 3 3xTF32 (tcgen05)
+std::atomic<long> g_mixed_gemm{3};
+std::atomic<long> g_reduction{1};     // 1: one-stage resident sytrd + ormtr; 2: two-stage sy2sb + sb2st
+std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (16, 32, 64)    // FP32 GEMMs of the mixed solve: 0 CUDA cores, 1 TF32, 3 3xTF32 (tcgen05)
 std::atomic<long long> g_launches{0};
 thread_local long long t_launches = 0;  // this thread's launches: a graph capture counts its own, not other threads'
 
@@ -279,6 +281,79 @@ void stage_ormtr(Call& k, int n, int m, const T* a, int lda, const T* tau, T* z,
   k.check(ormtr_upper<T>(n, m, a, lda, tau, z, ldz, nb, ormtr_carve<T>(w, n, m, nb), k.c->arena, k.s, tc), "ormtr");
 }
 
+// Tridiagonal reduction of f (n x n full symmetric, ld n; overwritten) to d (n), e (n-1), keeping what the
+// back-transformation z <- Q z needs: one stage (resident sytrd, then ormtr) or two stages (sy2sb + sb2st, then Q2 and
+// Q1).  Buffers are keyed by `pre` so that pipelines sharing a context keep separate workspaces.
+template <typename T>
+struct Reduction {
+  bool two = false;
+  int b = 0;
+  T* r = nullptr;    // one stage: LAPACK-layout reflectors
+  T* tau = nullptr;
+  T* v1 = nullptr;   // two stages
+  T* t1 = nullptr;
+  T* w2 = nullptr;
+};
+
+inline std::string key(const char* pre, const char* what) { return std::string(pre) + what; }
+
+template <typename T>
+bool two_stage_plan(Call& k, int n, int* b) {
+  if (g_reduction.load() != 2) return false;
+  *b = (int)g_band_width.load();
+  const size_t cap = k.c->max_smem;
+  return sy2sb_supported(n, *b, cap, (int)sizeof(T)) && sb2st_supported(n, *b, cap, (int)sizeof(T));
+}
+
+template <typename T>
+Reduction<T> stage_reduce(Call& k, const char* pre, int n, T* f, T* d, T* e, const TcGemm& tc) {
+  Reduction<T> red;
+  int b = 0;
+  if (!k.ok()) return red;
+  if (!two_stage_plan<T>(k, n, &b)) {
+    red.r = k.template dev<T>(key(pre, "R").c_str(), (size_t)n * n);
+    red.tau = k.template dev<T>(key(pre, "tau").c_str(), (size_t)n);
+    if (!k.ok()) return red;
+    stage_sytrd<T>(k, n, f, n, red.r, n, d, e, red.tau);
+    k.mark("sytrd");
+    return red;
+  }
+  red.two = true;
+  red.b = b;
+  const size_t nn = (size_t)n * n;
+  const int np = n / b + 1;
+  red.v1 = k.template dev<T>(key(pre, "V1").c_str(), nn);
+  red.t1 = k.template dev<T>(key(pre, "T1").c_str(), (size_t)np * b * b);
+  T* tau1 = k.template dev<T>(key(pre, "tau1").c_str(), (size_t)n);
+  T* ab = k.template dev<T>(key(pre, "AB").c_str(), (size_t)2 * b * n);
+  red.w2 = k.template dev<T>(key(pre, "W2").c_str(), nn);
+  T* work = k.template dev<T>(key(pre, "sbwork").c_str(), sy2sb_work_elems<T>(n, b));
+  if (!k.ok()) return red;
+  k.check(sy2sb<T>(n, b, f, n, red.v1, red.t1, tau1, ab, work, k.c->arena, tc, k.s), "sy2sb");
+  k.mark("sy2sb");
+  if (k.ok()) k.check(sb2st<T>(n, b, ab, d, e, red.w2, k.c->max_smem, k.c->d_status, wait_limit_ns(), k.s), "sb2st");
+  k.mark("sb2st");
+  return red;
+}
+
+template <typename T>
+void stage_backtransform(Call& k, const char* pre, int n, int m, const Reduction<T>& red, T* z, int ldz,
+                         const TcGemm& tc) {
+  if (!k.ok()) return;
+  if (!red.two) {
+    stage_ormtr<T>(k, n, m, red.r, n, red.tau, z, ldz, tc);
+    k.mark("ormtr");
+    return;
+  }
+  T* tq = k.template dev<T>(key(pre, "TQ").c_str(), q2_tq_elems(n, red.b));
+  T* w = k.template dev<T>(key(pre, "q1work").c_str(), q1_work_elems<T>(n, red.b, m));
+  if (!k.ok()) return;
+  k.check(q2_apply<T>(n, red.b, m, red.w2, z, ldz, tq, k.c->arena, k.c->max_smem, k.s), "Q2 back-transform");
+  k.mark("q2");
+  if (k.ok()) k.check(q1_apply<T>(n, red.b, m, red.v1, red.t1, z, ldz, w, k.c->arena, tc, k.s), "Q1 back-transform");
+  k.mark("q1");
+}
+
 // The tcgen05 engine for the FP32 GEMMs of an n x n mixed solve (passes from the mixed_gemm option; 0 = CUDA cores).
 TcGemm tc_engine(Call& k, int n) {
   TcGemm tc;
@@ -315,10 +390,8 @@ void core_sygvd_fp64(Call& k, int n, double* h, double* u, double* c, double* w)
   double* x = k.template dev<double>("gv.X", (size_t)n * n);
   double* t = k.template dev<double>("gv.T", (size_t)n * n);
   double* hp = k.template dev<double>("gv.Hp", (size_t)n * n);
-  double* r = k.template dev<double>("gv.R", (size_t)n * n);
   double* z = k.template dev<double>("gv.Z", (size_t)n * n);
   double* e = k.template dev<double>("gv.e", (size_t)n);
-  double* tau = k.template dev<double>("gv.tau", (size_t)n);
   if (!k.ok()) return;
   unsigned* pctr = k.template dev<unsigned>("potrf.ctr", 64);
   if (k.ok())
@@ -332,12 +405,10 @@ void core_sygvd_fp64(Call& k, int n, double* h, double* u, double* c, double* w)
   if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "congruence 2");
   if (k.ok()) symmetrize_upper<double>(n, hp, n, h, n, k.s);
   k.mark("congruence");
-  stage_sytrd<double>(k, n, h, n, r, n, w, e, tau);
-  k.mark("sytrd");
+  const Reduction<double> red = stage_reduce<double>(k, "gv.", n, h, w, e, TcGemm());
   stage_stedc(k, n, w, e, z, n);
   k.mark("stedc");
-  stage_ormtr<double>(k, n, n, r, n, tau, z, n);
-  k.mark("ormtr");
+  stage_backtransform<double>(k, "gv.", n, n, red, z, n, TcGemm());
   // C = X Z (X upper).
   p = gemm_problem<double>(n, n, n, 1.0, x, n, 0, z, n, 0, 0.0, c, n, kTriAUpper);
   if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "back-transform");
@@ -355,7 +426,7 @@ void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w
   double* sf = k.template dev<double>("mx.S", nn);
   double* z = k.template dev<double>("gv.Z", nn);
   double* e = k.template dev<double>("gv.e", (size_t)n);
-  float* f = k.template dev<float>("mx.f32", 5 * nn + 3 * (size_t)n);
+  float* f = k.template dev<float>("mx.f32", 5 * nn + 2 * (size_t)n);
   double* rw = k.template dev<double>("mx.refine", refine_work_elems(n));
   unsigned* pctr = k.template dev<unsigned>("potrf.ctr", 64);
   if (!k.ok()) return;
@@ -366,7 +437,6 @@ void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w
   float* zf = rf + nn;
   float* df = zf + nn;
   float* ef = df + n;
-  float* tauf = ef + n;
   const TcGemm tc = tc_engine(k, n);
   if (!k.ok()) return;
   symmetrize_upper<double>(n, u, n, sf, n, k.s);
@@ -381,8 +451,7 @@ void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w
   if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "congruence 2 (fp32)");
   if (k.ok()) symmetrize_upper<float>(n, rf, n, hf, n, k.s);
   k.mark("congruence");
-  stage_sytrd<float>(k, n, hf, n, rf, n, df, ef, tauf);
-  k.mark("sytrd");
+  const Reduction<float> red = stage_reduce<float>(k, "mx.", n, hf, df, ef, tc);
   if (k.ok()) {
     convert_f32_to_f64(n, df, w, k.s);
     convert_f32_to_f64(n, ef, e, k.s);
@@ -390,8 +459,7 @@ void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w
   stage_stedc(k, n, w, e, z, n);
   k.mark("stedc");
   if (k.ok()) convert_mat_f64_to_f32(n, n, z, n, zf, n, k.s);
-  stage_ormtr<float>(k, n, n, rf, n, tauf, zf, n, tc);
-  k.mark("ormtr");
+  stage_backtransform<float>(k, "mx.", n, n, red, zf, n, tc);
   p = gemm_problem<float>(n, n, n, 1.f, xf, n, 0, zf, n, 0, 0.f, tf, n, kTriAUpper);
   if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "back-transform (fp32)");
   if (k.ok()) convert_mat_f32_to_f64(n, n, tf, n, c, n, k.s);
@@ -409,16 +477,12 @@ void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
 // Standard problem on device buffers: f (n x n full symmetric, ld n) consumed; z (n x n) eigenvectors; w eigenvalues.
 void core_syevd(Call& k, int n, double* f, double* z, double* w, bool vectors) {
   if (!k.ok() || n <= 0) return;
-  double* r = k.template dev<double>("ev.R", (size_t)n * n);
   double* e = k.template dev<double>("ev.e", (size_t)n);
-  double* tau = k.template dev<double>("ev.tau", (size_t)n);
   if (!k.ok()) return;
-  stage_sytrd<double>(k, n, f, n, r, n, w, e, tau);
-  k.mark("sytrd");
+  const Reduction<double> red = stage_reduce<double>(k, "ev.", n, f, w, e, TcGemm());
   stage_stedc(k, n, w, e, z, n);
   k.mark("stedc");
-  if (vectors) stage_ormtr<double>(k, n, n, r, n, tau, z, n);
-  k.mark("ormtr");
+  if (vectors) stage_backtransform<double>(k, "ev.", n, n, red, z, n, TcGemm());
 }
 
 int info_of(int code, const DeviceStatus& st, int n) {
@@ -1108,6 +1172,16 @@ int xtb_gpu_set_option(const char* name, long value) {
     g_mixed_gemm = value;
     return 0;
   }
+  if (!std::strcmp(name, "reduction")) {
+    if (value != 1 && value != 2) return -2;
+    g_reduction = value;
+    return 0;
+  }
+  if (!std::strcmp(name, "band_width")) {
+    if (value != 16 && value != 32 && value != 64) return -2;
+    g_band_width = value;
+    return 0;
+  }
   return -1;
 }
 
@@ -1122,6 +1196,8 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "precision")) return g_precision;
   if (!std::strcmp(name, "refine_iters")) return g_refine_iters;
   if (!std::strcmp(name, "mixed_gemm")) return g_mixed_gemm;
+  if (!std::strcmp(name, "reduction")) return g_reduction;
+  if (!std::strcmp(name, "band_width")) return g_band_width;
   return -1;
 }
 

@@ -129,6 +129,32 @@ template <typename T>
 cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, int ldz, int nb, OrmtrWork<T> w,
                         DescArena& arena, cudaStream_t s, const TcGemm& tc = TcGemm());
 
+// ---------------------------------------------------------------------------------------------------- two-stage
+// Stage 1 (sy2sb.cu): a (n x n, full symmetric, lda) -> band of width b in a's lower triangle and in band storage ab
+// (ld 2b: diagonals 0 .. b, then zeros); explicit reflectors of every panel in v1 (n x n), their T factors in t1
+// (b x b per panel), tau1 (n).  work: sy2sb_work_elems.  Then z (n x m) <- Q1 z with q1_apply.
+bool sy2sb_supported(int n, int b, size_t max_smem, int elem_bytes);
+template <typename T>
+size_t sy2sb_work_elems(int n, int b);
+template <typename T>
+cudaError_t sy2sb(int n, int b, T* a, int lda, T* v1, T* t1, T* tau1, T* ab, T* work, DescArena& arena,
+                  const TcGemm& tc, cudaStream_t s);
+template <typename T>
+size_t q1_work_elems(int n, int b, int m);
+template <typename T>
+cudaError_t q1_apply(int n, int b, int m, const T* v1, const T* t1, T* z, int ldz, T* work, DescArena& arena,
+                     const TcGemm& tc, cudaStream_t s);
+// Stage 2 (sb2st.cu): band ab (ld 2b, n columns; read only) -> tridiagonal d (n), e (n-1) by bulge chasing on one
+// thread-block cluster; reflectors in w2 (n x n).  Then z (n x m) <- Q2 z with q2_apply (tq: q2_tq_elems scratch).
+bool sb2st_supported(int n, int b, size_t max_smem, int elem_bytes);
+size_t q2_tq_elems(int n, int b);
+template <typename T>
+cudaError_t sb2st(int n, int b, const T* ab, T* d, T* e, T* w2, size_t max_smem, DeviceStatus* st, uint64_t limit_ns,
+                  cudaStream_t s);
+template <typename T>
+cudaError_t q2_apply(int n, int b, int m, const T* w2, T* z, int ldz, T* tq, DescArena& arena, size_t max_smem,
+                     cudaStream_t s);
+
 // ---------------------------------------------------------------------------------------------------- stedc
 struct StedcWork;  // opaque, sized by stedc_work_bytes
 size_t stedc_work_bytes(int n);
