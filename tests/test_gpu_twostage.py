@@ -87,7 +87,7 @@ def test_mixed_two_stage(two, n):
     """Mixed precision through the two-stage reduction.  Its trailing updates run as 3xTF32 tensor-core GEMMs, whose
     operand representation (about 2^-21 per product against FP32's 2^-24) compounds over the panels, so the FP32
     vectors start about ten times less accurate than the one-stage path's.  Two refinement steps still meet the
-    north-star bars (eigenvalues <= 1e-10 Eh, density <= 1e-9); S-orthogonality lands near 1e-9 at n = 130, so its
+    mixed path's accuracy targets (eigenvalues <= 1e-10 Eh, density <= 1e-9); S-orthogonality lands near 1e-9 at n = 130, so its
     bar here is 5e-9."""
     two.set_option("precision", 32)
     h, s, lam = inputs.generalized(n, seed=70 + n)
