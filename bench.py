@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--batch-count", type=int, default=256, help="uneven batch size (0: skip the batch section)")
     ap.add_argument("--batch-steps", type=int, default=3)
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision section")
+    ap.add_argument("--no-autotune", action="store_true", help="use the default plan instead of autotuning it")
+    ap.add_argument("--no-two-stage", action="store_true", help="skip the two-stage reduction section")
     return ap.parse_args()
 
 
@@ -288,6 +290,51 @@ def run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush):
     return out
 
 
+def run_variant_section(args, dev, stream, H0, S0, lam_t, flush, options, steps=3):
+    """The n = 1788 solve under other library options (e.g. the two-stage reduction): mean ms over `steps` timed
+    solves after 3 warm-ups, stage times of one untimed solve, eigenvalue error against the exact spectrum."""
+    import torch
+
+    import xtbeig
+
+    n = H0.shape[0]
+    H, S = torch.empty_like(H0), torch.empty_like(S0)
+    W = torch.empty(n, dtype=torch.float64, device=dev)
+    old = {k: xtbeig.get_option(k) for k in options}
+
+    def solve():
+        H.copy_(H0)
+        S.copy_(S0)
+        info = xtbeig.dsygvd_device(n, H.data_ptr(), n, S.data_ptr(), n, W.data_ptr(), stream.cuda_stream)
+        if info != 0:
+            raise RuntimeError(f"xtb_dsygvd_device info={info}: {xtbeig.last_error()}")
+
+    try:
+        for k, v in options.items():
+            xtbeig.set_option(k, v)
+        for _ in range(3):
+            solve()
+        torch.cuda.synchronize(dev)
+        err = float((W - lam_t).abs().max())
+        xtbeig.set_option("stage_timing", 1)
+        solve()
+        stages = xtbeig.stage_times()
+        xtbeig.set_option("stage_timing", 0)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            solve()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+        ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+    finally:
+        for k, v in old.items():
+            xtbeig.set_option(k, v)
+    return {"options": options, "ms": round(ms, 4), "steps": steps, "warmup": 3, "eigenvalue_error_vs_exact": err,
+            "stages_ms": {k: round(v, 4) for k, v in stages}}
+
+
 def batch_sizes(count, seed=3, lo=124, hi=1788):
     """Sizes of the uneven batch: integers uniform in [lo, hi] from numpy's default_rng(seed)."""
     import numpy as np
@@ -442,6 +489,16 @@ def run_ours(args):
         if info != 0:
             raise RuntimeError(f"xtb_dsygvd_device info={info}: {xtbeig.last_error()}")
 
+    # Autotuning (outside every timed region): the fastest plan of each precision for this size.
+    plans = None
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        plans = {"fp64": xtbeig.autotune(n, 64, stream.cuda_stream)}
+        if not args.no_mixed:
+            plans["mixed"] = xtbeig.autotune(n, 32, stream.cuda_stream)
+        plans["tuning_s"] = round(time.perf_counter() - t0, 2)
+        xtbeig.set_option("autotune", 1)
+
     for _ in range(max(3, args.warmup)):
         solve()
     torch.cuda.synchronize(dev)
@@ -522,6 +579,14 @@ def run_ours(args):
     mixed = run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush) if not args.no_mixed else None
     if mixed:
         mixed["speedup_vs_fp64"] = round(ms_step_max / mixed["ms"], 3)
+    two_stage = None
+    if not args.no_two_stage:
+        two_stage = {"fp64": run_variant_section(args, dev, stream, H0, S0, lam_t, flush,
+                                                 {"autotune": 0, "reduction": 2, "band_width": 32})}
+        if not args.no_mixed:
+            two_stage["mixed"] = run_variant_section(args, dev, stream, H0, S0, lam_t, flush,
+                                                     {"autotune": 0, "reduction": 2, "band_width": 32,
+                                                      "precision": 32})
     batch = run_batch_section(args, dev, stream) if args.batch_count > 0 else None
 
     if rank == 0:
@@ -559,7 +624,9 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "clocks": clocks,
             "fp64_accuracy": acc64,
+            "plans": plans,
             "mixed": mixed,
+            "two_stage": two_stage,
             "batch": batch,
         }
         print(json.dumps(line), flush=True)

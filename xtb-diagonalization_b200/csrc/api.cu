@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cctype>
+#include <cmath>
 #include <condition_variable>
 #include <cstdio>
 #include <cstring>
@@ -33,9 +34,62 @@ std::atomic<long> g_graphs{1};
 std::atomic<long> g_batch_workers{4};
 std::atomic<long> g_precision{64};    // 64: FP64 throughout; 32: FP32 reduction chain + FP64 refinement
 std::atomic<long> g_refine_iters{2};
-std::atomic<long> g_mixed_gemm{3};
+std::atomic<long> g_mixed_gemm{3};    // FP32 GEMMs of the mixed solve: 0 CUDA cores, 1 TF32, 3 3xTF32 (tcgen05)
 std::atomic<long> g_reduction{1};     // 1: one-stage resident sytrd + ormtr; 2: two-stage sy2sb + sb2st
-std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (16, 32, 64)    // FP32 GEMMs of the mixed solve: 0 CUDA cores, 1 TF32, 3 3xTF32 (tcgen05)
+std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (16, 32, 64)
+std::atomic<long> g_autotune{0};      // 1: solves use the autotuned plan nearest their size (xtb_gpu_autotune)
+
+// The tunable choices of one solve.  A solve resolves its plan once (options, or the autotuned table) and every stage
+// reads it from t_plan; the plan's signature is part of the graph-cache key, so a captured graph is never replayed
+// under another plan.
+struct Plan {
+  int reduction = 1;   // 1 one-stage, 2 two-stage
+  int band = 32;       // two-stage band width
+  int sytrd_grid = 0;  // CTAs of the resident reduction (0: one per SM)
+  int ormtr_nb = 128;  // reflectors per compact-WY block of ormtr
+  int mixed_gemm = 3;  // FP32 GEMM engine of the mixed path
+  double ms = 0.0;     // measured time of the tuned plan
+  long long sig() const {
+    return (long long)reduction | (long long)band << 4 | (long long)sytrd_grid << 12 | (long long)ormtr_nb << 24 |
+           (long long)mixed_gemm << 36;
+  }
+};
+
+std::mutex g_plan_mu;
+std::map<std::pair<int, int>, Plan> g_plans;  // (precision, n) -> tuned plan
+thread_local Plan t_plan;
+thread_local const Plan* t_force_plan = nullptr;  // the autotuner's candidate under test
+
+Plan options_plan() {
+  Plan p;
+  p.reduction = (int)g_reduction.load();
+  p.band = (int)g_band_width.load();
+  p.sytrd_grid = (int)g_sytrd_grid.load();
+  p.ormtr_nb = (int)g_ormtr_nb.load();
+  p.mixed_gemm = (int)g_mixed_gemm.load();
+  return p;
+}
+
+// The plan of a solve of size n: the autotuner's candidate while it measures, else the tuned plan of the nearest
+// tuned size (log scale) when the autotune option is on, else the options.
+Plan plan_for(int n, int precision) {
+  if (t_force_plan) return *t_force_plan;
+  if (g_autotune.load()) {
+    std::lock_guard<std::mutex> lock(g_plan_mu);
+    const Plan* best = nullptr;
+    double dist = 0.0;
+    for (const auto& kv : g_plans) {
+      if (kv.first.first != precision) continue;
+      const double d = std::fabs(std::log((double)std::max(n, 1) / (double)kv.first.second));
+      if (!best || d < dist) {
+        best = &kv.second;
+        dist = d;
+      }
+    }
+    if (best) return *best;
+  }
+  return options_plan();
+}
 std::atomic<long long> g_launches{0};
 thread_local long long t_launches = 0;  // this thread's launches: a graph capture counts its own, not other threads'
 
@@ -241,7 +295,7 @@ template <typename T>
 void stage_sytrd(Call& k, int n, const T* dfull, int ldf, T* dout, int lda, T* d, T* e, T* tau) {
   if (!k.ok() || n <= 0) return;
   const size_t smem_cap = k.c->max_smem > 2048 ? k.c->max_smem - 2048 : k.c->max_smem;
-  SytrdPlan pl = sytrd_plan<T>(n, k.c->num_sms, smem_cap, (int)g_sytrd_grid.load());
+  SytrdPlan pl = sytrd_plan<T>(n, k.c->num_sms, smem_cap, t_plan.sytrd_grid);
   if (!pl.supported) {
     k.check(cudaErrorInvalidValue, "sytrd: size not supported");
     return;
@@ -275,7 +329,10 @@ void stage_sytrd(Call& k, int n, const T* dfull, int ldf, T* dout, int lda, T* d
 template <typename T>
 void stage_ormtr(Call& k, int n, int m, const T* a, int lda, const T* tau, T* z, int ldz, const TcGemm& tc = TcGemm()) {
   if (!k.ok() || n <= 1 || m <= 0) return;
-  const int nb = (int)std::max<long>(16, g_ormtr_nb.load());
+  // The compact-WY factor of a block is built in shared memory ((nb^2 + nb) elements): clamp nb to what fits.
+  int nbmax = 16;
+  while ((size_t)((nbmax + 16) * (nbmax + 16) + nbmax + 16) * sizeof(T) + 1024 <= k.c->max_smem) nbmax += 16;
+  const int nb = std::min(std::max(16, t_plan.ormtr_nb), nbmax);
   T* w = k.template dev<T>("ormtr.work", ormtr_work_elems<T>(n, m, nb));
   if (!k.ok()) return;
   k.check(ormtr_upper<T>(n, m, a, lda, tau, z, ldz, nb, ormtr_carve<T>(w, n, m, nb), k.c->arena, k.s, tc), "ormtr");
@@ -299,8 +356,8 @@ inline std::string key(const char* pre, const char* what) { return std::string(p
 
 template <typename T>
 bool two_stage_plan(Call& k, int n, int* b) {
-  if (g_reduction.load() != 2) return false;
-  *b = (int)g_band_width.load();
+  if (t_plan.reduction != 2) return false;
+  *b = t_plan.band;
   const size_t cap = k.c->max_smem;
   return sy2sb_supported(n, *b, cap, (int)sizeof(T)) && sb2st_supported(n, *b, cap, (int)sizeof(T));
 }
@@ -357,7 +414,7 @@ void stage_backtransform(Call& k, const char* pre, int n, int m, const Reduction
 // The tcgen05 engine for the FP32 GEMMs of an n x n mixed solve (passes from the mixed_gemm option; 0 = CUDA cores).
 TcGemm tc_engine(Call& k, int n) {
   TcGemm tc;
-  tc.passes = (int)g_mixed_gemm.load();
+  tc.passes = t_plan.mixed_gemm;
   if (tc.passes == 0) return tc;
   tc.work_elems = tc_work_elems(n);
   tc.work = k.template dev<float>("tc.work", tc.work_elems);
@@ -470,6 +527,7 @@ void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w
 }
 
 void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
+  t_plan = plan_for(n, (int)g_precision.load());
   if (g_precision.load() == 32) core_sygvd_mixed(k, n, h, u, c, w);
   else core_sygvd_fp64(k, n, h, u, c, w);
 }
@@ -477,6 +535,7 @@ void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
 // Standard problem on device buffers: f (n x n full symmetric, ld n) consumed; z (n x n) eigenvectors; w eigenvalues.
 void core_syevd(Call& k, int n, double* f, double* z, double* w, bool vectors) {
   if (!k.ok() || n <= 0) return;
+  t_plan = plan_for(n, 64);
   double* e = k.template dev<double>("ev.e", (size_t)n);
   if (!k.ok()) return;
   const Reduction<double> red = stage_reduce<double>(k, "ev.", n, f, w, e, TcGemm());
@@ -518,6 +577,7 @@ void sytrd_host(const int* n_, T* a, const int* lda_, T* d, T* e, T* tau, bool f
     if (full) copy_matrix<T>(n, n, da, lda, df, n, k.s);
     else symmetrize_upper<T>(n, da, lda, df, n, k.s);
   }
+  t_plan = plan_for(n, sizeof(T) == 4 ? 32 : 64);
   stage_sytrd<T>(k, n, df, n, da, lda, dd, de, dt);
   k.d2h(a, da, sizeof(T) * (size_t)lda * n, "D2H A");
   k.d2h(d, dd, sizeof(T) * n, "D2H d");
@@ -545,6 +605,7 @@ void ormtr_host(const int* n_, const int* m_, const T* a, const int* lda_, const
   k.h2d(da, a, sizeof(T) * (size_t)lda * n, "H2D A");
   k.h2d(dt, tau, sizeof(T) * (n - 1), "H2D tau");
   k.h2d(dz, z, sizeof(T) * (size_t)ldz * m, "H2D Z");
+  t_plan = plan_for(n, sizeof(T) == 4 ? 32 : 64);
   stage_ormtr<T>(k, n, m, da, lda, dt, dz, ldz);
   k.d2h(z, dz, sizeof(T) * (size_t)ldz * m, "D2H Z");
   k.finish();
@@ -733,7 +794,7 @@ void sygvd_device_body(Call& k, int n, double* a, int lda, double* b, int ldb, d
 int sygvd_device(Context* c, cudaStream_t s, int n, double* a, int lda, double* b, int ldb, double* w) {
   const std::vector<long long> key = {1, n, (long long)(uintptr_t)a, lda, (long long)(uintptr_t)b, ldb,
                                       (long long)(uintptr_t)w, (long long)(uintptr_t)s, g_precision.load(),
-                                      g_refine_iters.load()};
+                                      g_refine_iters.load(), plan_for(n, (int)g_precision.load()).sig()};
   DeviceStatus st{};
   const int code = run_graphed(c, s, key, &st, [&](Call& k) { sygvd_device_body(k, n, a, lda, b, ldb, w); });
   return info_of(code, st, n);
@@ -986,7 +1047,7 @@ int xtb_dsyevd_device(int n, double* a, int lda, double* w, void* stream) {
   Context* c = context();
   if (!c) return t_state.last_code;
   const std::vector<long long> key = {2, n, (long long)(uintptr_t)a, lda, (long long)(uintptr_t)w,
-                                      (long long)(uintptr_t)stream};
+                                      (long long)(uintptr_t)stream, plan_for(n, 64).sig()};
   DeviceStatus st{};
   const int code = run_graphed(c, (cudaStream_t)stream, key, &st, [&](Call& k) {
     double* df = k.dev<double>("dv.F", (size_t)n * n);
@@ -1053,6 +1114,124 @@ int xtb_sgemm_tc_device(int transa, int transb, int m, int n, int k_, float alph
   if (k.ok()) k.check(umma_gemm_group(&p, 1, passes, w, we, c0->d_status, wait_limit_ns(), k.s), "tcgen05 sgemm");
   DeviceStatus st{};
   return k.finish(&st);
+}
+
+int xtb_gpu_autotune(int n, int precision, void* stream) {
+  if (n < 1) return -1;
+  if (precision != 64 && precision != 32) return -2;
+  Context* c = context();
+  if (!c) return t_state.last_code;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!s) s = c->stream;  // graphs need a non-default stream
+  const size_t nn = (size_t)n * n;
+  double *h0, *s0, *h, *sb, *w;
+  {
+    Call k(c, s, true);
+    h0 = k.dev<double>("tune.H0", nn);
+    s0 = k.dev<double>("tune.S0", nn);
+    h = k.dev<double>("tune.H", nn);
+    sb = k.dev<double>("tune.S", nn);
+    w = k.dev<double>("tune.W", (size_t)n);
+    if (k.ok()) synthetic_pair(n, h0, s0, 0x5eedu + (unsigned)n, k.s);
+    const int code = k.finish();
+    if (code != 0) return code;
+  }
+  // Candidates, one coordinate at a time: the reduction (one stage with the resident kernel on all / 3/4 / 1/2 of the
+  // SMs; two stages with band width 16 / 32 / 64), then ormtr's block size for the one-stage winner, then the FP32
+  // GEMM engine of the mixed path.
+  const long prec0 = g_precision.load();
+  g_precision = precision;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    g_precision = prec0;
+    record(-1000, "autotune: event creation failed");
+    return -1000;
+  }
+  auto measure = [&](const Plan& cand) -> double {
+    t_force_plan = &cand;
+    double best = -1.0;
+    for (int rep = 0; rep < 6; ++rep) {  // eager, captured, then timed replays
+      if (cudaMemcpyAsync(h, h0, nn * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+          cudaMemcpyAsync(sb, s0, nn * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+          cudaEventRecord(e0, s) != cudaSuccess) {
+        best = -1.0;
+        break;
+      }
+      const int info = sygvd_device(c, s, n, h, n, sb, n, w);
+      cudaEventRecord(e1, s);
+      if (info != 0 || cudaEventSynchronize(e1) != cudaSuccess) {
+        best = -1.0;
+        break;
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep >= 2 && (best < 0.0 || ms < best)) best = ms;
+    }
+    t_force_plan = nullptr;
+    return best;
+  };
+  const Plan base = options_plan();
+  Plan best = base;
+  best.ms = -1.0;
+  auto consider = [&](Plan cand) {
+    const double ms = measure(cand);
+    if (ms > 0.0 && (best.ms < 0.0 || ms < best.ms)) {
+      best = cand;
+      best.ms = ms;
+    }
+  };
+  const int sms = c->num_sms;
+  for (int g : {0, (3 * sms) / 4, sms / 2}) {
+    Plan p = base;
+    p.reduction = 1;
+    p.sytrd_grid = g;
+    consider(p);
+  }
+  for (int b : {16, 32, 64}) {
+    if (!sy2sb_supported(n, b, c->max_smem, 8) || !sb2st_supported(n, b, c->max_smem, 8)) continue;
+    Plan p = base;
+    p.reduction = 2;
+    p.band = b;
+    consider(p);
+  }
+  if (best.reduction == 1) {
+    const Plan r = best;
+    for (int nb : {64, 256}) {
+      Plan p = r;
+      p.ormtr_nb = nb;
+      consider(p);
+    }
+  }
+  if (precision == 32) {
+    const Plan r = best;
+    Plan p = r;
+    p.mixed_gemm = r.mixed_gemm == 3 ? 0 : 3;
+    consider(p);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  g_precision = prec0;
+  if (best.ms < 0.0) {
+    record(-3, "autotune: no candidate plan completed");
+    return -3;
+  }
+  {
+    std::lock_guard<std::mutex> lock(g_plan_mu);
+    g_plans[{precision, n}] = best;
+  }
+  record(0, "");
+  return 0;
+}
+
+int xtb_gpu_tuned_plan(int n, int precision, char* buf, int len) {
+  std::lock_guard<std::mutex> lock(g_plan_mu);
+  auto it = g_plans.find({precision, n});
+  if (it == g_plans.end()) return -1;
+  const Plan& p = it->second;
+  const int w = std::snprintf(buf, buf && len > 0 ? (size_t)len : 0,
+                              "reduction=%d band_width=%d sytrd_grid=%d ormtr_nb=%d mixed_gemm=%d ms=%.4f",
+                              p.reduction, p.band, p.sytrd_grid, p.ormtr_nb, p.mixed_gemm, p.ms);
+  return w;
 }
 
 int xtb_dsygvd_batched(int count, const int* n, double* const* a, const int* lda, double* const* b, const int* ldb,
@@ -1182,6 +1361,11 @@ int xtb_gpu_set_option(const char* name, long value) {
     g_band_width = value;
     return 0;
   }
+  if (!std::strcmp(name, "autotune")) {
+    if (value != 0 && value != 1) return -2;
+    g_autotune = value;
+    return 0;
+  }
   return -1;
 }
 
@@ -1198,6 +1382,7 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "mixed_gemm")) return g_mixed_gemm;
   if (!std::strcmp(name, "reduction")) return g_reduction;
   if (!std::strcmp(name, "band_width")) return g_band_width;
+  if (!std::strcmp(name, "autotune")) return g_autotune;
   return -1;
 }
 

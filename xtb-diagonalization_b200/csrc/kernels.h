@@ -66,6 +66,9 @@ template <typename T>
 void set_identity(int n, T* a, int lda, cudaStream_t s);
 template <typename T>
 void zero_strict_lower(int n, T* a, int lda, cudaStream_t s);
+// A seeded synthetic generalized pair for timing: h random symmetric (entries in [-1, 1]), s = I + a symmetric banded
+// perturbation with |s_ij| <= 0.3 exp(-|i-j|/2) off the diagonal (strictly diagonally dominant, so positive definite).
+void synthetic_pair(int n, double* h, double* s, unsigned seed, cudaStream_t st);
 void convert_f32_to_f64(size_t count, const float* src, double* dst, cudaStream_t s);
 void convert_f64_to_f32(size_t count, const double* src, float* dst, cudaStream_t s);
 // Strided 2-D conversions (m x n, column-major).

@@ -1,6 +1,8 @@
 // Memory-shaped helper kernels: symmetrisation (the device side of xtb_dsymmetrize_pad, reference
 // Sources/Diagonalization/Exports.swift:117-138, there a CPU loop over 32 x 32 tiles), copies, precision conversion.
 // All are HBM/L2-bound; tiles are staged through shared memory so both the read and the transposed write coalesce.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace xtbeig {
@@ -209,5 +211,36 @@ template void set_identity<double>(int, double*, int, cudaStream_t);
 template void set_identity<float>(int, float*, int, cudaStream_t);
 template void zero_strict_lower<double>(int, double*, int, cudaStream_t);
 template void zero_strict_lower<float>(int, float*, int, cudaStream_t);
+
+namespace {
+
+__device__ __forceinline__ double hash_unit(unsigned seed, unsigned i, unsigned j) {
+  // splitmix-style integer hash of (seed, min(i,j), max(i,j)) -> [-1, 1)
+  unsigned long long x = ((unsigned long long)seed << 40) ^ ((unsigned long long)min(i, j) << 20) ^ max(i, j);
+  x += 0x9e3779b97f4a7c15ull;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  x ^= x >> 31;
+  return (double)(x >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+__global__ void synthetic_pair_kernel(int n, double* h, double* s, unsigned seed) {
+  const size_t total = (size_t)n * n;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % n), j = (int)(idx / n);
+    h[idx] = hash_unit(seed, (unsigned)i, (unsigned)j);
+    const int d = i > j ? i - j : j - i;
+    s[idx] = i == j ? 1.0 : 0.3 * exp(-0.5 * d) * hash_unit(seed ^ 0xa5a5a5a5u, (unsigned)i, (unsigned)j);
+  }
+}
+
+}  // namespace
+
+void synthetic_pair(int n, double* h, double* s, unsigned seed, cudaStream_t st) {
+  const size_t total = (size_t)n * n;
+  const int grid = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+  synthetic_pair_kernel<<<grid, 256, 0, st>>>(n, h, s, seed);
+  note_launches();
+}
 
 }  // namespace xtbeig

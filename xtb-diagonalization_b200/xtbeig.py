@@ -48,6 +48,8 @@ def lib():
         _lib.xtb_dsygvd_batched.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P]
         _lib.xtb_dsygvd_batched_device.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P]
         _lib.xtb_dsygvd_refine_device.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _I, _P]
+        _lib.xtb_gpu_autotune.argtypes = [_I, _I, _P]
+        _lib.xtb_gpu_tuned_plan.argtypes = [_I, _I, C.c_char_p, _I]
         _lib.xtb_sgemm_tc_device.argtypes = [_I, _I, _I, _I, _I, C.c_float, _P, _I, _P, _I, C.c_float, _P, _I, _I,
                                              _P]
         _lib.xtb_gpu_stage_name.restype = C.c_char_p
@@ -225,6 +227,26 @@ def dsygvd_refine_device(n, h_ptr, ldh, s_ptr, lds, c_ptr, ldc, w_ptr, iters=2, 
     """FP64 refinement of approximate generalized eigenvectors c (device buffers); returns info."""
     return int(lib().xtb_dsygvd_refine_device(int(n), _P(h_ptr), int(ldh), _P(s_ptr), int(lds), _P(c_ptr), int(ldc),
                                               _P(w_ptr), int(iters), _P(stream) if stream else None))
+
+
+def autotune(n: int, precision: int = 64, stream=0) -> dict:
+    """xtb_gpu_autotune: time the candidate plans for size n and keep the fastest; returns the tuned plan."""
+    rc = lib().xtb_gpu_autotune(n, precision, stream)
+    if rc != 0:
+        raise RuntimeError(f"xtb_gpu_autotune({n}, {precision}) returned {rc}: {last_error()}")
+    return tuned_plan(n, precision)
+
+
+def tuned_plan(n: int, precision: int = 64):
+    """The tuned plan of (n, precision) as a dict, or None if that size was not tuned."""
+    buf = C.create_string_buffer(256)
+    if lib().xtb_gpu_tuned_plan(n, precision, buf, 256) < 0:
+        return None
+    out = {}
+    for kv in buf.value.decode().split():
+        k, v = kv.split("=")
+        out[k] = float(v) if k == "ms" else int(v)
+    return out
 
 
 def sgemm_tc_device(transa, transb, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc, passes=3,
