@@ -105,6 +105,13 @@ int xtb_dsygvd_refine_device(int n, const double* h, int ldh, const double* s, i
 int xtb_sgemm_tc_device(int transa, int transb, int m, int n, int k, float alpha, const float* a, int lda,
                         const float* b, int ldb, float beta, float* c, int ldc, int passes, void* stream);
 
+/* FP64 GEMM on the FP64 tensor cores (DMMA), DEVICE pointers, column-major as BLAS dgemm: C = alpha op(A) op(B) +
+ * beta C.  The engine of every FP64 GEMM-shaped stage (congruence, ormtr, back-transform, refinement, D&C merges; the
+ * reference calls Accelerate dgemm for them, e.g. Sources/Diagonalization/Stages/WYTransform.swift:22-79).  Queued
+ * on `stream` and synchronised.  Returns 0, -(argument position), -1000 - cudaError, or a device status code. */
+int xtb_dgemm_device(int transa, int transb, int m, int n, int k, double alpha, const double* a, int lda,
+                     const double* b, int ldb, double beta, double* c, int ldc, void* stream);
+
 /* Autotuner, the measured replacement for the reference's fixed choice of band width by n (SBROptions.recommended,
  * Sources/Diagonalization/SBROptions.swift:73-82): times candidate plans for generalized solves of size n at the given
  * precision (64 or 32) on a seeded synthetic pair built on the device - the reduction (one stage on all, 3/4 or 1/2 of

@@ -93,3 +93,34 @@ def test_sgemm_argument_errors(xe):
     assert xe.sgemm_tc_device(0, 0, 4, 4, 4, 1.0, None, 3, None, 4, 0.0, None, 4, 3, 0) == -8
     assert xe.sgemm_tc_device(0, 0, 4, 4, 4, 1.0, None, 4, None, 4, 0.0, None, 4, 2, 0) == -14
     assert xe.sgemm_tc_device(0, 0, 0, 4, 4, 1.0, None, 4, None, 4, 0.0, None, 4, 3, 0) == 0
+
+
+def _run_d(xe, ta, tb, m, n, k, alpha, beta, seed):
+    import torch
+
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    ar, ac = (k, m) if ta else (m, k)
+    br, bc = (n, k) if tb else (k, n)
+    A = torch.randn((ac, ar), generator=g, dtype=torch.float64).to(dev)
+    B = torch.randn((bc, br), generator=g, dtype=torch.float64).to(dev)
+    C = torch.randn((n, m), generator=g, dtype=torch.float64).to(dev)
+    opa = A.T.T if ta else A.T
+    opb = B.T.T if tb else B.T
+    ref = alpha * (opa @ opb) + beta * C.T
+    absprod = opa.abs() @ opb.abs() + abs(beta) * C.T.abs()
+    torch.cuda.synchronize(dev)
+    rc = xe.dgemm_device(ta, tb, m, n, k, alpha, A.data_ptr(), ar, B.data_ptr(), br, beta, C.data_ptr(), m, 0)
+    torch.cuda.synchronize(dev)
+    assert rc == 0, (rc, xe.last_error())
+    return C.T, ref, absprod
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("mnk", [(1, 1, 1), (63, 65, 17), (130, 257, 129), (600, 500, 700)])
+def test_dgemm_matches_fp64(xe, ta, tb, mnk):
+    """xtb_dgemm_device (FP64 DMMA) against torch's FP64 product: elementwise within 2 k eps |op(A)| |op(B)|."""
+    m, n, k = mnk
+    out, ref, absprod = _run_d(xe, ta, tb, m, n, k, 1.25, -0.5, seed=m + 3 * n + 7 * k + ta + 2 * tb)
+    bound = 2 * (k + 2) * 2.0 ** -53 * absprod + 1e-300
+    assert bool(((out - ref).abs() <= bound).all())

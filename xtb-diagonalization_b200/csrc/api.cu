@@ -1116,6 +1116,26 @@ int xtb_sgemm_tc_device(int transa, int transb, int m, int n, int k_, float alph
   return k.finish(&st);
 }
 
+int xtb_dgemm_device(int transa, int transb, int m, int n, int k_, double alpha, const double* a, int lda,
+                     const double* b, int ldb, double beta, double* c, int ldc, void* stream) {
+  if (transa != 0 && transa != 1) return -1;
+  if (transb != 0 && transb != 1) return -2;
+  if (m < 0) return -3;
+  if (n < 0) return -4;
+  if (k_ < 0) return -5;
+  if (lda < std::max(1, transa ? k_ : m)) return -8;
+  if (ldb < std::max(1, transb ? n : k_)) return -10;
+  if (ldc < std::max(1, m)) return -13;
+  if (m == 0 || n == 0) return 0;
+  Context* c0 = context();
+  if (!c0) return t_state.last_code;
+  Call k(c0, (cudaStream_t)stream, true);
+  GemmDesc<double> p = gemm_problem<double>(m, n, k_, alpha, a, lda, transa, b, ldb, transb, beta, c, ldc);
+  k.check(gemm_group<double>(c0->arena, &p, 1, k.s), "dgemm");
+  DeviceStatus st{};
+  return k.finish(&st);
+}
+
 int xtb_gpu_autotune(int n, int precision, void* stream) {
   if (n < 1) return -1;
   if (precision != 64 && precision != 32) return -2;

@@ -49,6 +49,7 @@ def lib():
         _lib.xtb_dsygvd_batched_device.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P]
         _lib.xtb_dsygvd_refine_device.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _I, _P]
         _lib.xtb_gpu_autotune.argtypes = [_I, _I, _P]
+        _lib.xtb_dgemm_device.argtypes = [_I, _I, _I, _I, _I, C.c_double, _P, _I, _P, _I, C.c_double, _P, _I, _P]
         _lib.xtb_gpu_tuned_plan.argtypes = [_I, _I, C.c_char_p, _I]
         _lib.xtb_sgemm_tc_device.argtypes = [_I, _I, _I, _I, _I, C.c_float, _P, _I, _P, _I, C.c_float, _P, _I, _I,
                                              _P]
@@ -227,6 +228,11 @@ def dsygvd_refine_device(n, h_ptr, ldh, s_ptr, lds, c_ptr, ldc, w_ptr, iters=2, 
     """FP64 refinement of approximate generalized eigenvectors c (device buffers); returns info."""
     return int(lib().xtb_dsygvd_refine_device(int(n), _P(h_ptr), int(ldh), _P(s_ptr), int(lds), _P(c_ptr), int(ldc),
                                               _P(w_ptr), int(iters), _P(stream) if stream else None))
+
+
+def dgemm_device(transa, transb, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc, stream=0) -> int:
+    """xtb_dgemm_device: FP64 GEMM on the FP64 tensor cores on device pointers."""
+    return lib().xtb_dgemm_device(transa, transb, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc, stream)
 
 
 def autotune(n: int, precision: int = 64, stream=0) -> dict:
