@@ -108,6 +108,9 @@ struct Context {
   DeviceStatus* d_status = nullptr;
   DeviceStatus* h_status = nullptr;
   std::vector<cudaEvent_t> events;  // pool for stage timing
+  // Host-pointer solves overlap their transfers with compute on a second stream (created on first use).
+  cudaStream_t copy = nullptr;
+  cudaEvent_t ev_in_b = nullptr, ev_in_a = nullptr, ev_factor = nullptr, ev_out = nullptr;
   // Bumped whenever a buffer is reallocated: captured graphs hold raw buffer addresses and are only replayed while
   // the generation they were captured in is current.
   uint64_t generation = 0;
@@ -179,6 +182,8 @@ struct Call {
 
   std::vector<std::pair<const char*, cudaEvent_t>> marks;
   bool timing = false;
+  // Called by the generalized pipelines right after the Cholesky factor U is final and before the first read of H.
+  std::function<void(Call&)> after_factor;
 
   // Host-pointer calls run on the context's own stream; device-pointer calls on the caller's stream, where NULL is the
   // CUDA legacy default stream (ordered with the caller's other work on blocking streams).
@@ -455,6 +460,7 @@ void core_sygvd_fp64(Call& k, int n, double* h, double* u, double* c, double* w)
     k.check(potrf_inverse_upper(n, u, n, x, n, t, pctr, k.c->num_sms, k.c->d_status, wait_limit_ns(), k.s),
             "potrf+inverse");
   k.mark("potrf_inverse");
+  if (k.after_factor && k.ok()) k.after_factor(k);
   // G = H X (X upper), then H' = X^T G on the upper tiles, symmetrised for the reduction.
   GemmDesc<double> p = gemm_problem<double>(n, n, n, 1.0, h, n, 0, x, n, 0, 0.0, t, n, kTriBUpper);
   if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "congruence 1");
@@ -500,6 +506,7 @@ void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w
   k.check(potrf_inverse_upper(n, u, n, x, n, t, pctr, k.c->num_sms, k.c->d_status, wait_limit_ns(), k.s),
           "potrf+inverse");
   k.mark("potrf_inverse");
+  if (k.after_factor && k.ok()) k.after_factor(k);
   convert_mat_f64_to_f32(n, n, x, n, xf, n, k.s);
   convert_mat_f64_to_f32(n, n, h, n, hf, n, k.s);
   GemmDesc<float> p = gemm_problem<float>(n, n, n, 1.f, hf, n, 0, xf, n, 0, 0.f, tf, n, kTriBUpper);
@@ -522,7 +529,8 @@ void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w
   if (k.ok()) convert_mat_f32_to_f64(n, n, tf, n, c, n, k.s);
   k.mark("trmm");
   if (k.ok())
-    k.check(refine_generalized(n, h, n, sf, n, c, n, w, (int)g_refine_iters.load(), rw, k.c->arena, k.s), "refine");
+    k.check(refine_generalized(n, h, n, sf, n, u, n, c, n, w, (int)g_refine_iters.load(), rw, k.c->arena, k.s),
+            "refine");
   k.mark("refine");
 }
 
@@ -738,6 +746,18 @@ using namespace xtbeig;
 namespace {
 
 // dsygvd (itype 1, arguments already checked, n > 0) on the calling thread's context: host arrays in, results back.
+bool ensure_copy_stream(Context* c) {
+  if (c->copy) return true;
+  if (cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) return false;
+  for (cudaEvent_t* e : {&c->ev_in_b, &c->ev_in_a, &c->ev_factor, &c->ev_out})
+    if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return false;
+  return true;
+}
+
+// Host-pointer dsygvd.  The transfers overlap the compute on a second stream: B goes first (the Cholesky needs it),
+// A uploads while the Cholesky runs and is symmetrised only when the congruence needs it, and the factor U goes back to
+// the host while the reduction runs.  (With pageable host arrays the driver stages each copy and the overlap is
+// smaller; pinned arrays overlap fully.)
 int sygvd_host(char jz, char ul, int n, double* a, int lda, double* b, int ldb, double* w) {
   Context* c = context();
   if (!c) return t_state.last_code;
@@ -748,28 +768,47 @@ int sygvd_host(char jz, char ul, int n, double* a, int lda, double* b, int ldb, 
   double* du = k.dev<double>("io.U", (size_t)n * n);
   double* dc = k.dev<double>("io.C", (size_t)n * n);
   double* dw = k.dev<double>("io.w", n);
-  k.h2d(da, a, sizeof(double) * (size_t)lda * n, "H2D A");
-  k.h2d(db, b, sizeof(double) * (size_t)ldb * n, "H2D B");
+  if (k.ok() && !ensure_copy_stream(c)) k.check(cudaErrorUnknown, "copy stream");
+  cudaStream_t cs = c->copy;
   if (k.ok()) {
-    if (ul == 'U') {
-      symmetrize_upper<double>(n, da, lda, dh, n, k.s);
-      copy_matrix<double>(n, n, db, ldb, du, n, k.s);
-    } else {
-      symmetrize_lower<double>(n, da, lda, dh, n, k.s);
-      symmetrize_lower<double>(n, db, ldb, du, n, k.s);
+    // The copy stream starts after everything queued on the compute stream so far (buffer reuse across calls).
+    k.check(cudaEventRecord(c->ev_out, k.s), "event");
+    if (k.ok()) k.check(cudaStreamWaitEvent(cs, c->ev_out, 0), "wait");
+    if (k.ok()) k.check(cudaMemcpyAsync(db, b, sizeof(double) * (size_t)ldb * n, cudaMemcpyHostToDevice, cs), "H2D B");
+    if (k.ok()) k.check(cudaEventRecord(c->ev_in_b, cs), "event");
+    if (k.ok()) k.check(cudaMemcpyAsync(da, a, sizeof(double) * (size_t)lda * n, cudaMemcpyHostToDevice, cs), "H2D A");
+    if (k.ok()) k.check(cudaEventRecord(c->ev_in_a, cs), "event");
+    if (k.ok()) k.check(cudaStreamWaitEvent(k.s, c->ev_in_b, 0), "wait B");
+  }
+  if (k.ok()) {
+    if (ul == 'U') copy_matrix<double>(n, n, db, ldb, du, n, k.s);
+    else symmetrize_lower<double>(n, db, ldb, du, n, k.s);
+  }
+  k.after_factor = [&](Call& kk) {
+    // U is final: put it into the caller's triangle of B and send it back on the copy stream.
+    if (ul == 'U') copy_matrix<double>(n, n, du, n, db, ldb, kk.s);
+    else upper_transpose_to_lower<double>(n, du, n, db, ldb, kk.s);
+    kk.check(cudaEventRecord(c->ev_factor, kk.s), "event");
+    if (kk.ok()) kk.check(cudaStreamWaitEvent(cs, c->ev_factor, 0), "wait U");
+    if (kk.ok()) kk.check(cudaMemcpyAsync(b, db, sizeof(double) * (size_t)ldb * n, cudaMemcpyDeviceToHost, cs), "D2H B");
+    // H for the congruence.
+    if (kk.ok()) kk.check(cudaStreamWaitEvent(kk.s, c->ev_in_a, 0), "wait A");
+    if (kk.ok()) {
+      if (ul == 'U') symmetrize_upper<double>(n, da, lda, dh, n, kk.s);
+      else symmetrize_lower<double>(n, da, lda, dh, n, kk.s);
     }
-  }
+  };
   core_sygvd(k, n, dh, du, dc, dw);
-  // B <- the factor in the caller's triangle; the other triangle keeps its input (du's lower part is the input's).
-  if (k.ok()) {
-    if (ul == 'U') copy_matrix<double>(n, n, du, n, db, ldb, k.s);
-    else upper_transpose_to_lower<double>(n, du, n, db, ldb, k.s);
-  }
-  k.d2h(b, db, sizeof(double) * (size_t)ldb * n, "D2H B");
+  k.after_factor = nullptr;
   k.d2h(w, dw, sizeof(double) * n, "D2H w");
   if (jz == 'V' && k.ok())
     k.check(cudaMemcpy2DAsync(a, sizeof(double) * lda, dc, sizeof(double) * n, sizeof(double) * n, n,
                               cudaMemcpyDeviceToHost, k.s), "D2H C");
+  // The compute stream's completion covers the copy stream's work; after a failure, no copy may still be reading or
+  // writing the caller's arrays when the call returns.
+  if (k.ok()) k.check(cudaEventRecord(c->ev_out, cs), "event");
+  if (k.ok()) k.check(cudaStreamWaitEvent(k.s, c->ev_out, 0), "join");
+  if (!k.ok() && cs) cudaStreamSynchronize(cs);
   DeviceStatus st{};
   const int code = k.finish(&st);
   return info_of(code, st, n);
@@ -1086,7 +1125,7 @@ int xtb_dsygvd_refine_device(int n, const double* h, int ldh, const double* s, i
   if (k.ok()) {
     symmetrize_upper<double>(n, h, ldh, hf, n, k.s);
     symmetrize_upper<double>(n, s, lds, sf, n, k.s);
-    k.check(refine_generalized(n, hf, n, sf, n, c, ldc, w, iters, rw, c0->arena, k.s), "refine");
+    k.check(refine_generalized(n, hf, n, sf, n, nullptr, 0, c, ldc, w, iters, rw, c0->arena, k.s), "refine");
   }
   DeviceStatus st{};
   const int code = k.finish(&st);
