@@ -396,6 +396,29 @@ def run_batch_section(args, dev, stream):
     ms_batch = statistics.mean(a.elapsed_time(b) for a, b in ev)
     eig_err = max(float((W[i] - LAM[i]).abs().max()) for i in range(count))
 
+    # The same batch in mixed precision (FP32 reduction chain + FP64 refinement).
+    mixed = None
+    if not args.no_mixed:
+        prec0 = xtbeig.get_option("precision")
+        xtbeig.set_option("precision", 32)
+        try:
+            for _ in range(3):
+                batch_step()
+            torch.cuda.synchronize(dev)
+            evm = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+            for k in range(steps):
+                evm[k][0].record(stream)
+                batch_step()
+                evm[k][1].record(stream)
+            torch.cuda.synchronize(dev)
+            ms_m = statistics.mean(a.elapsed_time(b) for a, b in evm)
+            err_m = max(float((W[i] - LAM[i]).abs().max()) for i in range(count))
+        finally:
+            xtbeig.set_option("precision", prec0)
+        mixed = {"solves_per_s": round(count / (ms_m * 1e-3), 2), "ms_per_batch": round(ms_m, 2), "steps": steps,
+                 "warmup": 3, "speedup_vs_fp64_batch": round(ms_batch / ms_m, 3),
+                 "eigenvalue_error_vs_exact_max": err_m}
+
     # One at a time: each problem alone on the caller's stream (eager, captured, then the timed replay).
     per = []
     for i, n in enumerate(sizes):
@@ -448,6 +471,7 @@ def run_batch_section(args, dev, stream):
         "one_at_a_time_solves_per_s": round(count / (one_ms * 1e-3), 2), "one_at_a_time_ms": round(one_ms, 2),
         "speedup_vs_one_at_a_time": round(one_ms / ms_batch, 3), "per_size_ms_alone": bins,
         "eigenvalue_error_vs_exact_max": eig_err,
+        "mixed": mixed,
         "e2e": {"solves_per_s": round(count / e2e[0], 2), "ms_per_batch": round(e2e[0] * 1e3, 2),
                 "h2d_bytes_per_batch": 2 * elems * 8, "d2h_bytes_per_batch": (2 * elems + sum(sizes)) * 8},
         "l2": "not flushed: the batch's matrices (~%.1f GB) exceed L2" % (4 * elems * 8 / 1e9),

@@ -185,8 +185,10 @@ cudaError_t dk_adjoint(int n, const double* c, const double* e, double mu, doubl
 // FP64 Ogita-Aishima refinement of C (n x n, ldc) for H C = S C diag(w), C^T S C = I: `iters` steps, then c and w
 // rewritten in ascending eigenvalue order.  h, s full symmetric (FP64).  work: refine_work_elems(n) doubles.
 size_t refine_work_elems(int n);
-cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s, int lds, double* c, int ldc,
-                               double* w, int iters, double* work, DescArena& arena, cudaStream_t st);
+// u (may be NULL): the upper Cholesky factor of s (ld ldu); with it C^T S C is formed as (U C)^T (U C).
+cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s, int lds, const double* u, int ldu,
+                               double* c, int ldc, double* w, int iters, double* work, DescArena& arena,
+                               cudaStream_t st);
 
 // ---------------------------------------------------------------------------------------------------- helpers
 // Stage nprob descriptors through the arena (tile grid and tile_begin filled in from M, N) and launch one grouped GEMM.
