@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision section")
     ap.add_argument("--no-autotune", action="store_true", help="use the default plan instead of autotuning it")
     ap.add_argument("--no-two-stage", action="store_true", help="skip the two-stage reduction section")
+    ap.add_argument("--hs-bin", default=None, help="solve an H/S dump (hsbin format) instead of the synthetic pair")
     return ap.parse_args()
 
 
@@ -335,6 +336,48 @@ def run_variant_section(args, dev, stream, H0, S0, lam_t, flush, options, steps=
             "stages_ms": {k: round(v, 4) for k, v in stages}}
 
 
+def run_cycle_section(args, dev, stream, H0, S0, lam_t, flush, precision, steps=5):
+    """The per-SCC-cycle solve: S factored once (xtb_dsygvd_factor_device, untimed), then `steps` timed solves of the
+    same H with that factorization (xtb_dsygvd_factored_device: congruence, reduction, tridiagonal eigensolve,
+    back-transformations and, at precision 32, the refinement)."""
+    import torch
+
+    import xtbeig
+
+    n = H0.shape[0]
+    U = S0.clone()
+    X = torch.empty_like(S0)
+    H = torch.empty_like(H0)
+    W = torch.empty(n, dtype=torch.float64, device=dev)
+    prec0 = xtbeig.get_option("precision")
+    xtbeig.set_option("precision", precision)
+    try:
+        if xtbeig.dsygvd_factor_device(n, U.data_ptr(), n, X.data_ptr(), n, stream.cuda_stream) != 0:
+            raise RuntimeError(f"xtb_dsygvd_factor_device: {xtbeig.last_error()}")
+
+        def solve():
+            H.copy_(H0)
+            info = xtbeig.dsygvd_factored_device(n, H.data_ptr(), n, U.data_ptr(), n, X.data_ptr(), n, W.data_ptr(),
+                                                 stream.cuda_stream)
+            if info != 0:
+                raise RuntimeError(f"xtb_dsygvd_factored_device info={info}: {xtbeig.last_error()}")
+
+        for _ in range(3):
+            solve()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            solve()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+        ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+        err = float((W - lam_t).abs().max())
+    finally:
+        xtbeig.set_option("precision", prec0)
+    return {"ms": round(ms, 4), "steps": steps, "warmup": 3, "eigenvalue_error_vs_exact": err}
+
+
 def batch_sizes(count, seed=3, lo=124, hi=1788):
     """Sizes of the uneven batch: integers uniform in [lo, hi] from numpy's default_rng(seed)."""
     import numpy as np
@@ -498,8 +541,17 @@ def run_ours(args):
     n = args.n
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
-    H0, S0, lam_t = generalized_on_device(n, args.seed, dev)  # symmetric: row-major == column-major
-    lam = lam_t.cpu().numpy()
+    if args.hs_bin:
+        import hsbin
+
+        dump = hsbin.read_hs_bin(args.hs_bin)
+        n = args.n = dump["n"]
+        # symmetric: row-major == column-major
+        H0 = torch.from_numpy(np.ascontiguousarray(dump["h"])).to(dev)
+        S0 = torch.from_numpy(np.ascontiguousarray(dump["s"])).to(dev)
+        lam_t = None  # no exact spectrum: errors are reported against the FP64 GPU solve
+    else:
+        H0, S0, lam_t = generalized_on_device(n, args.seed, dev)  # symmetric: row-major == column-major
     h_np, s_np = H0.cpu().numpy(), S0.cpu().numpy()
     H = torch.empty_like(H0)
     S = torch.empty_like(S0)
@@ -526,6 +578,11 @@ def run_ours(args):
     for _ in range(max(3, args.warmup)):
         solve()
     torch.cuda.synchronize(dev)
+    eig_reference = "exact spectrum of the construction"
+    if lam_t is None:
+        lam_t = W.clone()
+        eig_reference = "FP64 GPU solve (the dump has no exact spectrum)"
+    lam = lam_t.cpu().numpy()
     # accuracy of the measured configuration (outside the timed region)
     w = W.cpu().numpy()
     eig_err = float(np.max(np.abs(w - lam)))
@@ -603,6 +660,10 @@ def run_ours(args):
     mixed = run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush) if not args.no_mixed else None
     if mixed:
         mixed["speedup_vs_fp64"] = round(ms_step_max / mixed["ms"], 3)
+    cycle = {"fp64": run_cycle_section(args, dev, stream, H0, S0, lam_t, flush, 64)}
+    if not args.no_mixed:
+        cycle["mixed"] = run_cycle_section(args, dev, stream, H0, S0, lam_t, flush, 32)
+        cycle["mixed_speedup_vs_fp64"] = round(cycle["fp64"]["ms"] / cycle["mixed"]["ms"], 3)
     two_stage = None
     if not args.no_two_stage:
         two_stage = {"fp64": run_variant_section(args, dev, stream, H0, S0, lam_t, flush,
@@ -630,7 +691,9 @@ def run_ours(args):
             "warmup": max(3, args.warmup), "ms_per_step": round(ms_step_max, 4), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generalized H, S; exact spectrum known)",
-            "config": {"workload": f"generalized eigensolve n={n} seed={args.seed}, all eigenpairs, FP64 path",
+            "config": {"workload": (f"generalized eigensolve of {os.path.basename(args.hs_bin)} n={n}" if args.hs_bin else
+                                    f"generalized eigensolve n={n} seed={args.seed}") + ", all eigenpairs, FP64 path",
+                       "eigenvalue_reference": eig_reference,
                        "path": "potrf, trtri, X^T H X, resident sytrd, D&C stedc, WY ormtr, X C' (all CUDA)",
                        "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}",
                        "eigenvalue_error_vs_exact": eig_err, "wall_s_timed_region": round(t_wall, 3)},
@@ -649,6 +712,7 @@ def run_ours(args):
             "clocks": clocks,
             "fp64_accuracy": acc64,
             "plans": plans,
+            "scc_cycle": cycle,
             "mixed": mixed,
             "two_stage": two_stage,
             "batch": batch,

@@ -87,6 +87,18 @@ int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, 
 #define XTB_NOALLOC_MAX_N 1792
 int xtb_dsytrd_upper_noalloc(int n, double* a, int lda, double* d, double* e, double* tau, void* stream);
 
+/* Per-geometry / per-SCC-cycle split of xtb_dsygvd_device, for xTB's loop in which S is fixed per geometry and H
+ * changes every cycle (the reference factors S once per geometry, mctc_potrf, and reduces each cycle with the
+ * congruence of scripts/kernels/congruence.c:33-52).  xtb_dsygvd_factor_device: b (S's upper triangle, ldb) <- U with
+ * S = U^T U (the strict lower triangle is not touched), x (n x n, ldx) <- U^-1 (upper, strict lower part zero); returns
+ * info as dsygvd (n + i for a non-SPD S).  xtb_dsygvd_factored_device: solves H C = S C diag(w) with that
+ * factorization - congruence, reduction, tridiagonal eigensolve, back-transformations (and, at precision 32, the FP64
+ * refinement against S = U^T U) - without refactoring S; a (H's upper triangle, lda) <- C.  Same results as
+ * xtb_dsygvd_device on the same inputs.  Device pointers; queued on `stream`. */
+int xtb_dsygvd_factor_device(int n, double* b, int ldb, double* x, int ldx, void* stream);
+int xtb_dsygvd_factored_device(int n, double* a, int lda, const double* u, int ldu, const double* x, int ldx,
+                               double* w, void* stream);
+
 /* FP64 refinement of an approximate generalized eigendecomposition on DEVICE pointers: h, s (upper triangles, ldh,
  * lds), c (n x n, ldc) approximate eigenvectors in ascending eigenvalue order (e.g. an FP32 solve, or the previous
  * SCC cycle's C), w receives the eigenvalues.  `iters` Ogita-Aishima steps in the S inner product (the reference's refinement,

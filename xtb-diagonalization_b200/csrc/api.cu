@@ -445,26 +445,32 @@ void stage_stedc(Call& k, int n, double* d, double* e, double* z, int ldz) {
   if (k.ok()) ready = true;
 }
 
-// The generalized core on device buffers: h (n x n, full symmetric, ld n) is consumed; u (n x n, ld n) holds B's upper
-// triangle on entry and U on exit; c (n x n, ld n) receives C; w (n) the eigenvalues.
-void core_sygvd_fp64(Call& k, int n, double* h, double* u, double* c, double* w) {
+// The Cholesky factorization of a generalized solve: u (S's upper triangle, ld ldu) <- U with S = U^T U (the strict
+// lower triangle is not touched); x (ld ldx) <- U^-1 (upper, strict lower part zero).
+void stage_factor(Call& k, int n, double* u, int ldu, double* x, int ldx) {
   if (!k.ok() || n <= 0) return;
-  double* x = k.template dev<double>("gv.X", (size_t)n * n);
+  double* t = k.template dev<double>("gv.T", (size_t)n * n);
+  unsigned* pctr = k.template dev<unsigned>("potrf.ctr", 64);
+  if (k.ok())
+    k.check(potrf_inverse_upper(n, u, ldu, x, ldx, t, pctr, k.c->num_sms, k.c->d_status, wait_limit_ns(), k.s),
+            "potrf+inverse");
+  k.mark("potrf_inverse");
+  if (k.after_factor && k.ok()) k.after_factor(k);
+}
+
+// The generalized solve after the factorization (FP64): h (n x n, full symmetric, ld n) is consumed; u = U, x = U^-1
+// (upper, from stage_factor); c (n x n, ld n) receives C; w (n) the eigenvalues.
+void solve_factored_fp64(Call& k, int n, double* h, const double* x, int ldx, double* c, double* w) {
+  if (!k.ok() || n <= 0) return;
   double* t = k.template dev<double>("gv.T", (size_t)n * n);
   double* hp = k.template dev<double>("gv.Hp", (size_t)n * n);
   double* z = k.template dev<double>("gv.Z", (size_t)n * n);
   double* e = k.template dev<double>("gv.e", (size_t)n);
   if (!k.ok()) return;
-  unsigned* pctr = k.template dev<unsigned>("potrf.ctr", 64);
-  if (k.ok())
-    k.check(potrf_inverse_upper(n, u, n, x, n, t, pctr, k.c->num_sms, k.c->d_status, wait_limit_ns(), k.s),
-            "potrf+inverse");
-  k.mark("potrf_inverse");
-  if (k.after_factor && k.ok()) k.after_factor(k);
   // G = H X (X upper), then H' = X^T G on the upper tiles, symmetrised for the reduction.
-  GemmDesc<double> p = gemm_problem<double>(n, n, n, 1.0, h, n, 0, x, n, 0, 0.0, t, n, kTriBUpper);
+  GemmDesc<double> p = gemm_problem<double>(n, n, n, 1.0, h, n, 0, x, ldx, 0, 0.0, t, n, kTriBUpper);
   if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "congruence 1");
-  p = gemm_problem<double>(n, n, n, 1.0, x, n, 1, t, n, 0, 0.0, hp, n, kTriALower | kCUpper);
+  p = gemm_problem<double>(n, n, n, 1.0, x, ldx, 1, t, n, 0, 0.0, hp, n, kTriALower | kCUpper);
   if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "congruence 2");
   if (k.ok()) symmetrize_upper<double>(n, hp, n, h, n, k.s);
   k.mark("congruence");
@@ -473,25 +479,22 @@ void core_sygvd_fp64(Call& k, int n, double* h, double* u, double* c, double* w)
   k.mark("stedc");
   stage_backtransform<double>(k, "gv.", n, n, red, z, n, TcGemm());
   // C = X Z (X upper).
-  p = gemm_problem<double>(n, n, n, 1.0, x, n, 0, z, n, 0, 0.0, c, n, kTriAUpper);
+  p = gemm_problem<double>(n, n, n, 1.0, x, ldx, 0, z, n, 0, 0.0, c, n, kTriAUpper);
   if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "back-transform");
   k.mark("trmm");
 }
 
-// Mixed precision: the reduction chain in FP32 (congruence, resident sytrd, ormtr, back-transform; the tridiagonal
-// eigensolve and the Cholesky factor in FP64), then FP64 Ogita-Aishima refinement on the FP64 pair (H, S).  Same
-// buffer contract as core_sygvd (h is kept intact here).
-void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w) {
+// Mixed precision after the factorization: the reduction chain in FP32 (congruence, reduction, back-transformations;
+// the tridiagonal eigensolve in FP64), then FP64 Ogita-Aishima refinement on the FP64 pair (H, S = U^T U), with
+// C^T S C formed as (U C)^T (U C).  h is kept intact here.
+void solve_factored_mixed(Call& k, int n, double* h, const double* u, int ldu, const double* x, int ldx, double* c,
+                          double* w) {
   if (!k.ok() || n <= 0) return;
   const size_t nn = (size_t)n * n;
-  double* x = k.template dev<double>("gv.X", nn);
-  double* t = k.template dev<double>("gv.T", nn);
-  double* sf = k.template dev<double>("mx.S", nn);
   double* z = k.template dev<double>("gv.Z", nn);
   double* e = k.template dev<double>("gv.e", (size_t)n);
   float* f = k.template dev<float>("mx.f32", 5 * nn + 2 * (size_t)n);
   double* rw = k.template dev<double>("mx.refine", refine_work_elems(n));
-  unsigned* pctr = k.template dev<unsigned>("potrf.ctr", 64);
   if (!k.ok()) return;
   float* xf = f;
   float* hf = xf + nn;
@@ -502,12 +505,7 @@ void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w
   float* ef = df + n;
   const TcGemm tc = tc_engine(k, n);
   if (!k.ok()) return;
-  symmetrize_upper<double>(n, u, n, sf, n, k.s);
-  k.check(potrf_inverse_upper(n, u, n, x, n, t, pctr, k.c->num_sms, k.c->d_status, wait_limit_ns(), k.s),
-          "potrf+inverse");
-  k.mark("potrf_inverse");
-  if (k.after_factor && k.ok()) k.after_factor(k);
-  convert_mat_f64_to_f32(n, n, x, n, xf, n, k.s);
+  convert_mat_f64_to_f32(n, n, x, ldx, xf, n, k.s);
   convert_mat_f64_to_f32(n, n, h, n, hf, n, k.s);
   GemmDesc<float> p = gemm_problem<float>(n, n, n, 1.f, hf, n, 0, xf, n, 0, 0.f, tf, n, kTriBUpper);
   if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "congruence 1 (fp32)");
@@ -529,15 +527,27 @@ void core_sygvd_mixed(Call& k, int n, double* h, double* u, double* c, double* w
   if (k.ok()) convert_mat_f32_to_f64(n, n, tf, n, c, n, k.s);
   k.mark("trmm");
   if (k.ok())
-    k.check(refine_generalized(n, h, n, sf, n, u, n, c, n, w, (int)g_refine_iters.load(), rw, k.c->arena, k.s),
+    k.check(refine_generalized(n, h, n, nullptr, 0, u, ldu, c, n, w, (int)g_refine_iters.load(), rw, k.c->arena,
+                               k.s),
             "refine");
   k.mark("refine");
 }
 
-void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
+// Generalized solve given the factorization (u = U, x = U^-1): h consumed, c <- C, w <- eigenvalues.
+void core_sygvd_factored(Call& k, int n, double* h, const double* u, int ldu, const double* x, int ldx, double* c,
+                         double* w) {
   t_plan = plan_for(n, (int)g_precision.load());
-  if (g_precision.load() == 32) core_sygvd_mixed(k, n, h, u, c, w);
-  else core_sygvd_fp64(k, n, h, u, c, w);
+  if (g_precision.load() == 32) solve_factored_mixed(k, n, h, u, ldu, x, ldx, c, w);
+  else solve_factored_fp64(k, n, h, x, ldx, c, w);
+}
+
+// The generalized core on device buffers: h (n x n, full symmetric, ld n) is consumed; u (n x n, ld n) holds B's upper
+// triangle on entry and U on exit; c (n x n, ld n) receives C; w (n) the eigenvalues.
+void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
+  if (!k.ok() || n <= 0) return;
+  double* x = k.template dev<double>("gv.X", (size_t)n * n);
+  stage_factor(k, n, u, n, x, n);
+  core_sygvd_factored(k, n, h, u, n, x, n, c, w);
 }
 
 // Standard problem on device buffers: f (n x n full symmetric, ld n) consumed; z (n x n) eigenvectors; w eigenvalues.
@@ -1106,6 +1116,44 @@ int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, 
   Context* c = context();
   if (!c) return t_state.last_code;
   return sygvd_device(c, (cudaStream_t)stream, n, a, lda, b, ldb, w);
+}
+
+int xtb_dsygvd_factor_device(int n, double* b, int ldb, double* x, int ldx, void* stream) {
+  if (n < 0) return -1;
+  if (ldb < std::max(1, n)) return -3;
+  if (ldx < std::max(1, n)) return -5;
+  if (n == 0) return 0;
+  Context* c = context();
+  if (!c) return t_state.last_code;
+  const std::vector<long long> key = {3, n, (long long)(uintptr_t)b, ldb, (long long)(uintptr_t)x, ldx,
+                                      (long long)(uintptr_t)stream};
+  DeviceStatus st{};
+  const int code = run_graphed(c, (cudaStream_t)stream, key, &st, [&](Call& k) { stage_factor(k, n, b, ldb, x, ldx); });
+  return info_of(code, st, n);
+}
+
+int xtb_dsygvd_factored_device(int n, double* a, int lda, const double* u, int ldu, const double* x, int ldx,
+                               double* w, void* stream) {
+  if (n < 0) return -1;
+  if (lda < std::max(1, n)) return -3;
+  if (ldu < std::max(1, n)) return -5;
+  if (ldx < std::max(1, n)) return -7;
+  if (n == 0) return 0;
+  Context* c = context();
+  if (!c) return t_state.last_code;
+  const std::vector<long long> key = {4, n, (long long)(uintptr_t)a, lda, (long long)(uintptr_t)u, ldu,
+                                      (long long)(uintptr_t)x, ldx, (long long)(uintptr_t)w,
+                                      (long long)(uintptr_t)stream, g_precision.load(), g_refine_iters.load(),
+                                      plan_for(n, (int)g_precision.load()).sig()};
+  DeviceStatus st{};
+  const int code = run_graphed(c, (cudaStream_t)stream, key, &st, [&](Call& k) {
+    double* dh = k.dev<double>("dv.F", (size_t)n * n);
+    double* dc = k.dev<double>("dv.C", (size_t)n * n);
+    if (k.ok()) symmetrize_upper<double>(n, a, lda, dh, n, k.s);
+    core_sygvd_factored(k, n, dh, u, ldu, x, ldx, dc, w);
+    if (k.ok()) copy_matrix<double>(n, n, dc, n, a, lda, k.s);
+  });
+  return info_of(code, st, n);
 }
 
 int xtb_dsygvd_refine_device(int n, const double* h, int ldh, const double* s, int lds, double* c, int ldc,

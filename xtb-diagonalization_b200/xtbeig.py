@@ -49,6 +49,8 @@ def lib():
         _lib.xtb_dsygvd_batched_device.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P]
         _lib.xtb_dsygvd_refine_device.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _I, _P]
         _lib.xtb_gpu_autotune.argtypes = [_I, _I, _P]
+        _lib.xtb_dsygvd_factor_device.argtypes = [_I, _P, _I, _P, _I, _P]
+        _lib.xtb_dsygvd_factored_device.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _P]
         _lib.xtb_dgemm_device.argtypes = [_I, _I, _I, _I, _I, C.c_double, _P, _I, _P, _I, C.c_double, _P, _I, _P]
         _lib.xtb_gpu_tuned_plan.argtypes = [_I, _I, C.c_char_p, _I]
         _lib.xtb_sgemm_tc_device.argtypes = [_I, _I, _I, _I, _I, C.c_float, _P, _I, _P, _I, C.c_float, _P, _I, _I,
@@ -228,6 +230,16 @@ def dsygvd_refine_device(n, h_ptr, ldh, s_ptr, lds, c_ptr, ldc, w_ptr, iters=2, 
     """FP64 refinement of approximate generalized eigenvectors c (device buffers); returns info."""
     return int(lib().xtb_dsygvd_refine_device(int(n), _P(h_ptr), int(ldh), _P(s_ptr), int(lds), _P(c_ptr), int(ldc),
                                               _P(w_ptr), int(iters), _P(stream) if stream else None))
+
+
+def dsygvd_factor_device(n, b_ptr, ldb, x_ptr, ldx, stream=0) -> int:
+    """xtb_dsygvd_factor_device: S = U^T U in place (U in b's upper triangle) and X = U^-1, on device pointers."""
+    return lib().xtb_dsygvd_factor_device(n, b_ptr, ldb, x_ptr, ldx, stream)
+
+
+def dsygvd_factored_device(n, a_ptr, lda, u_ptr, ldu, x_ptr, ldx, w_ptr, stream=0) -> int:
+    """xtb_dsygvd_factored_device: the generalized solve with a factorization from dsygvd_factor_device."""
+    return lib().xtb_dsygvd_factored_device(n, a_ptr, lda, u_ptr, ldu, x_ptr, ldx, w_ptr, stream)
 
 
 def dgemm_device(transa, transb, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc, stream=0) -> int:
