@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision section")
     ap.add_argument("--no-autotune", action="store_true", help="use the default plan instead of autotuning it")
     ap.add_argument("--no-two-stage", action="store_true", help="skip the two-stage reduction section")
+    ap.add_argument("--adjoint-count", type=int, default=32, help="problems of the density-adjoint section (0: skip)")
     ap.add_argument("--hs-bin", default=None, help="solve an H/S dump (hsbin format) instead of the synthetic pair")
     return ap.parse_args()
 
@@ -378,6 +379,51 @@ def run_cycle_section(args, dev, stream, H0, S0, lam_t, flush, precision, steps=
     return {"ms": round(ms, 4), "steps": steps, "warmup": 3, "eigenvalue_error_vs_exact": err}
 
 
+def run_adjoint_section(args, dev):
+    """The differentiation workload: `count` generalized problems at n = 588 (problem i built on the device with seed
+    4000 + i), Fermi occupations at T = 300 K with mu at mid-gap, W symmetric standard normal; dL/dH and dL/dS of
+    L = sum(W o P) through xtb_dsygvd_density_adjoint_batched (host arrays: each problem's solve, eigenvectors and
+    adjoint on the GPU, nothing stored), timed end to end in FP64 and in mixed precision."""
+    import numpy as np
+    import torch
+
+    import xtbeig
+    from oracle import fermi
+
+    count, n = args.adjoint_count, 588
+    hs, ss, mus, wbs = [], [], [], []
+    rng = np.random.default_rng(4)
+    for i in range(count):
+        h, s, lam = generalized_on_device(n, 4000 + i, dev)
+        hs.append(np.asfortranarray(h.cpu().numpy()))
+        ss.append(np.asfortranarray(s.cpu().numpy()))
+        lam = lam.cpu().numpy()
+        mus.append(0.5 * (lam[n // 2 - 1] + lam[n // 2]))
+        w = rng.standard_normal((n, n))
+        wbs.append(np.asfortranarray(w + w.T))
+    kts = [fermi.kt_of(300.0)] * count
+    out = {"count": count, "n": n, "temperature_K": 300.0}
+    prec0 = xtbeig.get_option("precision")
+    try:
+        for name, prec in (("fp64", 64), ("mixed", 32)):
+            if prec == 32 and args.no_mixed:
+                continue
+            xtbeig.set_option("precision", prec)
+            xtbeig.density_adjoint_batched(hs, ss, kts, mus, wbs)  # warm-up: every worker's context and buffers
+            t0 = time.perf_counter()
+            _, _, info = xtbeig.density_adjoint_batched(hs, ss, kts, mus, wbs)
+            dt = time.perf_counter() - t0
+            if np.any(info != 0):
+                raise RuntimeError(f"adjoint batch info {info}")
+            out[name] = {"ms_per_batch": round(dt * 1e3, 2), "problems_per_s": round(count / dt, 2)}
+    finally:
+        xtbeig.set_option("precision", prec0)
+    if "mixed" in out:
+        out["mixed_speedup_vs_fp64"] = round(out["fp64"]["ms_per_batch"] / out["mixed"]["ms_per_batch"], 3)
+    out["note"] = "end to end through the C ABI from host arrays (H, S, W in; dL/dH, dL/dS out); accuracy is tested"
+    return out
+
+
 def batch_sizes(count, seed=3, lo=124, hi=1788):
     """Sizes of the uneven batch: integers uniform in [lo, hi] from numpy's default_rng(seed)."""
     import numpy as np
@@ -673,6 +719,7 @@ def run_ours(args):
                                                      {"autotune": 0, "reduction": 2, "band_width": 32,
                                                       "precision": 32})
     batch = run_batch_section(args, dev, stream) if args.batch_count > 0 else None
+    adjoint = run_adjoint_section(args, dev) if args.adjoint_count > 0 else None
 
     if rank == 0:
         peak, peak_kind = load_peaks()
@@ -716,6 +763,7 @@ def run_ours(args):
             "mixed": mixed,
             "two_stage": two_stage,
             "batch": batch,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

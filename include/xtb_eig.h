@@ -160,6 +160,16 @@ int xtb_dsygvd_density_adjoint(int n, const double* h, int ldh, const double* s,
                                const double* wbar, int ldw, double* dh, int lddh, double* ds, int ldds, double* w_out,
                                double* c_out, int ldc);
 
+/* A batch of density adjoints (host arrays): problem i is xtb_dsygvd_density_adjoint(n[i], h[i], ldh[i], s[i],
+ * lds[i], kt[i], mu[i], wbar[i], ldw[i], dh[i], lddh[i], ds[i], ldds[i]) with its eigenpairs recomputed on the GPU
+ * (nothing is stored between problems), spread over the batch workers like xtb_dsygvd_batched.  info[i] per problem
+ * (info may be NULL).  Returns 0, the info of the lowest-numbered failing problem, -1 for count < 0, or -2 for a NULL
+ * array or an invalid n / leading dimension / kt (nothing is computed then). */
+int xtb_dsygvd_density_adjoint_batched(int count, const int* n, const double* const* h, const int* ldh,
+                                       const double* const* s, const int* lds, const double* kt, const double* mu,
+                                       const double* const* wbar, const int* ldw, double* const* dh,
+                                       const int* lddh, double* const* ds, const int* ldds, int* info);
+
 /* Options (process-wide): "sytrd_grid" (CTAs of the resident reduction, 0 = auto), "ormtr_nb" (reflectors per
  * compact-WY block, default 128), "wait_limit_ms" (device wait time limit, default 2000), "stage_timing" (1: record
  * CUDA events at stage boundaries; read with xtb_gpu_stage_*), "graphs" (default 1: a device-pointer solve repeated

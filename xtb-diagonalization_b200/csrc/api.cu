@@ -1435,6 +1435,27 @@ int xtb_dsygvd_density_adjoint(int n, const double* h, int ldh, const double* s,
   return info_of(code, st, n);
 }
 
+int xtb_dsygvd_density_adjoint_batched(int count, const int* n, const double* const* h, const int* ldh,
+                                       const double* const* s, const int* lds, const double* kt, const double* mu,
+                                       const double* const* wbar, const int* ldw, double* const* dh,
+                                       const int* lddh, double* const* ds, const int* ldds, int* info) {
+  if (count < 0) return -1;
+  if (count == 0) return 0;
+  if (!n || !h || !ldh || !s || !lds || !kt || !mu || !wbar || !ldw || !dh || !lddh || !ds || !ldds) return -2;
+  for (int i = 0; i < count; ++i) {
+    const int m = n[i];
+    if (m < 0 || ldh[i] < std::max(1, m) || lds[i] < std::max(1, m) || ldw[i] < std::max(1, m) ||
+        lddh[i] < std::max(1, m) || ldds[i] < std::max(1, m) || !(kt[i] > 0.0))
+      return -2;
+    if (m > 0 && (!h[i] || !s[i] || !wbar[i] || !dh[i] || !ds[i])) return -2;
+  }
+  return run_batch(count, n, info, [&](int i) {
+    return n[i] == 0 ? 0
+                     : xtb_dsygvd_density_adjoint(n[i], h[i], ldh[i], s[i], lds[i], kt[i], mu[i], wbar[i], ldw[i],
+                                                  dh[i], lddh[i], ds[i], ldds[i], nullptr, nullptr, 0);
+  });
+}
+
 int xtb_gpu_set_option(const char* name, long value) {
   if (!name) return -1;
   if (!std::strcmp(name, "sytrd_grid")) { g_sytrd_grid = value; return 0; }

@@ -49,6 +49,7 @@ def lib():
         _lib.xtb_dsygvd_batched_device.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P]
         _lib.xtb_dsygvd_refine_device.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _I, _P]
         _lib.xtb_gpu_autotune.argtypes = [_I, _I, _P]
+        _lib.xtb_dsygvd_density_adjoint_batched.argtypes = [_I] + [_P] * 14
         _lib.xtb_dsygvd_factor_device.argtypes = [_I, _P, _I, _P, _I, _P]
         _lib.xtb_dsygvd_factored_device.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _P]
         _lib.xtb_dgemm_device.argtypes = [_I, _I, _I, _I, _I, C.c_double, _P, _I, _P, _I, C.c_double, _P, _I, _P]
@@ -325,6 +326,26 @@ def density_adjoint(h, s, kt, mu, wbar):
 
 
 # ---------------------------------------------------------------------------------------------- convenience
+
+
+def density_adjoint_batched(hs, ss, kts, mus, wbars):
+    """xtb_dsygvd_density_adjoint_batched on lists of host arrays: returns (list of dL/dH, list of dL/dS, infos)."""
+    count = len(hs)
+    hs = [np.asfortranarray(h, dtype=np.float64) for h in hs]
+    ss = [np.asfortranarray(s, dtype=np.float64) for s in ss]
+    ws = [np.asfortranarray(w, dtype=np.float64) for w in wbars]
+    ns = np.array([h.shape[0] for h in hs], np.int32)
+    dhs = [np.zeros((m, m), order="F") for m in ns]
+    dss = [np.zeros((m, m), order="F") for m in ns]
+    arr = lambda xs: (C.c_void_p * count)(*[x.ctypes.data for x in xs])
+    kt = np.asarray(kts, np.float64)
+    mu = np.asarray(mus, np.float64)
+    info = np.zeros(count, np.int32)
+    rc = lib().xtb_dsygvd_density_adjoint_batched(count, _p(ns), arr(hs), _p(ns), arr(ss), _p(ns), _p(kt), _p(mu),
+                                                  arr(ws), _p(ns), arr(dhs), _p(ns), arr(dss), _p(ns), _p(info))
+    if rc < 0:
+        raise RuntimeError(f"xtb_dsygvd_density_adjoint_batched returned {rc}: {last_error()}")
+    return dhs, dss, info
 
 def sytrd_upper(a, dtype=np.float64):
     """Functional form: returns (A_out, d, e, tau) like oracle.lapack.sytrd_upper."""
