@@ -111,6 +111,9 @@ struct Context {
   // Host-pointer solves overlap their transfers with compute on a second stream (created on first use).
   cudaStream_t copy = nullptr;
   cudaEvent_t ev_in_b = nullptr, ev_in_a = nullptr, ev_factor = nullptr, ev_out = nullptr;
+  // Work that runs beside the main chain (ormtr's preparation during the tridiagonal eigensolve).
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // Bumped whenever a buffer is reallocated: captured graphs hold raw buffer addresses and are only replayed while
   // the generation they were captured in is current.
   uint64_t generation = 0;
@@ -265,6 +268,8 @@ struct Call {
                     "status read");
     cudaError_t se = cudaStreamSynchronize(s);
     if (ok() && se != cudaSuccess) check(se, "synchronize");
+    // Side-stream work is joined into s on every normal path; after an early failure it may still run: wait for it.
+    if (c->aux) cudaStreamSynchronize(c->aux);
     if (!ok()) {
       record(-1000 - (int)err, std::string("CUDA error at ") + where + ": " + cudaGetErrorString(err));
       return -1000 - (int)err;
@@ -331,13 +336,19 @@ void stage_sytrd(Call& k, int n, const T* dfull, int ldf, T* dout, int lda, T* d
   k.check(cudaMemsetAsync(ctr, 0, 64 * sizeof(unsigned), k.s), "sytrd counter");  if (k.ok()) k.check(sytrd_launch<T>(p, pl, k.s), "sytrd launch");
 }
 
+// ormtr's compact-WY block size: the plan's, clamped so that a block's factor ((nb^2 + nb) elements) fits in shared
+// memory.
+template <typename T>
+int ormtr_block(Call& k) {
+  int nbmax = 16;
+  while ((size_t)((nbmax + 16) * (nbmax + 16) + nbmax + 16) * sizeof(T) + 1024 <= k.c->max_smem) nbmax += 16;
+  return std::min(std::max(16, t_plan.ormtr_nb), nbmax);
+}
+
 template <typename T>
 void stage_ormtr(Call& k, int n, int m, const T* a, int lda, const T* tau, T* z, int ldz, const TcGemm& tc = TcGemm()) {
   if (!k.ok() || n <= 1 || m <= 0) return;
-  // The compact-WY factor of a block is built in shared memory ((nb^2 + nb) elements): clamp nb to what fits.
-  int nbmax = 16;
-  while ((size_t)((nbmax + 16) * (nbmax + 16) + nbmax + 16) * sizeof(T) + 1024 <= k.c->max_smem) nbmax += 16;
-  const int nb = std::min(std::max(16, t_plan.ormtr_nb), nbmax);
+  const int nb = ormtr_block<T>(k);
   T* w = k.template dev<T>("ormtr.work", ormtr_work_elems<T>(n, m, nb));
   if (!k.ok()) return;
   k.check(ormtr_upper<T>(n, m, a, lda, tau, z, ldz, nb, ormtr_carve<T>(w, n, m, nb), k.c->arena, k.s, tc), "ormtr");
@@ -352,6 +363,9 @@ struct Reduction {
   int b = 0;
   T* r = nullptr;    // one stage: LAPACK-layout reflectors
   T* tau = nullptr;
+  bool prepared = false;  // one stage: ormtr's V, T, Y being built on the aux stream (joined before the apply)
+  int nb = 0;
+  OrmtrWork<T> ow{};
   T* v1 = nullptr;   // two stages
   T* t1 = nullptr;
   T* w2 = nullptr;
@@ -367,8 +381,18 @@ bool two_stage_plan(Call& k, int n, int* b) {
   return sy2sb_supported(n, *b, cap, (int)sizeof(T)) && sb2st_supported(n, *b, cap, (int)sizeof(T));
 }
 
+bool ensure_aux_stream(Context* c) {
+  if (c->aux) return true;
+  if (cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) return false;
+  return cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) == cudaSuccess;
+}
+
+// `back`: the caller will back-transform n columns, so the one-stage path starts ormtr's preparation (V, T, Y from the
+// reflectors) on the aux stream right after the reduction, overlapping the tridiagonal eigensolve; stage_backtransform
+// joins it.
 template <typename T>
-Reduction<T> stage_reduce(Call& k, const char* pre, int n, T* f, T* d, T* e, const TcGemm& tc) {
+Reduction<T> stage_reduce(Call& k, const char* pre, int n, T* f, T* d, T* e, const TcGemm& tc, bool back = true) {
   Reduction<T> red;
   int b = 0;
   if (!k.ok()) return red;
@@ -378,6 +402,25 @@ Reduction<T> stage_reduce(Call& k, const char* pre, int n, T* f, T* d, T* e, con
     if (!k.ok()) return red;
     stage_sytrd<T>(k, n, f, n, red.r, n, d, e, red.tau);
     k.mark("sytrd");
+    if (back && n > 1 && k.ok()) {
+      red.nb = ormtr_block<T>(k);
+      T* w = k.template dev<T>("ormtr.work", ormtr_work_elems<T>(n, n, red.nb));
+      if (!k.ok()) return red;
+      red.ow = ormtr_carve<T>(w, n, n, red.nb);
+      if (!ensure_aux_stream(k.c)) {
+        k.check(cudaErrorUnknown, "aux stream");
+        return red;
+      }
+      k.check(cudaEventRecord(k.c->ev_fork, k.s), "fork");
+      if (!k.ok()) return red;
+      k.check(cudaStreamWaitEvent(k.c->aux, k.c->ev_fork, 0), "fork wait");
+      if (k.ok())
+        k.check(ormtr_prepare<T>(n, red.r, n, red.tau, red.nb, red.ow, k.c->arena, k.c->aux, tc), "ormtr prepare");
+      // Joined in stage_backtransform; recorded even after a failure so that a capture can always be closed.
+      const cudaError_t je = cudaEventRecord(k.c->ev_join, k.c->aux);
+      if (k.ok()) k.check(je, "join record");
+      red.prepared = true;
+    }
     return red;
   }
   red.two = true;
@@ -403,7 +446,12 @@ void stage_backtransform(Call& k, const char* pre, int n, int m, const Reduction
                          const TcGemm& tc) {
   if (!k.ok()) return;
   if (!red.two) {
-    stage_ormtr<T>(k, n, m, red.r, n, red.tau, z, ldz, tc);
+    if (red.prepared) {
+      k.check(cudaStreamWaitEvent(k.s, k.c->ev_join, 0), "join");
+      if (k.ok()) k.check(ormtr_apply<T>(n, m, z, ldz, red.nb, red.ow, k.c->arena, k.s, tc), "ormtr");
+    } else {
+      stage_ormtr<T>(k, n, m, red.r, n, red.tau, z, ldz, tc);
+    }
     k.mark("ormtr");
     return;
   }
@@ -528,7 +576,7 @@ void solve_factored_mixed(Call& k, int n, double* h, const double* u, int ldu, c
   k.mark("trmm");
   if (k.ok())
     k.check(refine_generalized(n, h, n, nullptr, 0, u, ldu, c, n, w, (int)g_refine_iters.load(), rw, k.c->arena,
-                               k.s),
+                               k.s, &tc),
             "refine");
   k.mark("refine");
 }
@@ -556,7 +604,7 @@ void core_syevd(Call& k, int n, double* f, double* z, double* w, bool vectors) {
   t_plan = plan_for(n, 64);
   double* e = k.template dev<double>("ev.e", (size_t)n);
   if (!k.ok()) return;
-  const Reduction<double> red = stage_reduce<double>(k, "ev.", n, f, w, e, TcGemm());
+  const Reduction<double> red = stage_reduce<double>(k, "ev.", n, f, w, e, TcGemm(), vectors);
   stage_stedc(k, n, w, e, z, n);
   k.mark("stedc");
   if (vectors) stage_backtransform<double>(k, "ev.", n, n, red, z, n, TcGemm());

@@ -131,6 +131,14 @@ OrmtrWork<T> ormtr_carve(T* base, int n, int m, int nb);
 template <typename T>
 cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, int ldz, int nb, OrmtrWork<T> w,
                         DescArena& arena, cudaStream_t s, const TcGemm& tc = TcGemm());
+// The two halves of ormtr_upper: prepare builds V, the T factors and Y = V T^T from the reflectors alone (so it can run
+// while the tridiagonal eigensolve produces Z); apply updates Z.
+template <typename T>
+cudaError_t ormtr_prepare(int n, const T* a, int lda, const T* tau, int nb, OrmtrWork<T> w, DescArena& arena,
+                          cudaStream_t s, const TcGemm& tc = TcGemm());
+template <typename T>
+cudaError_t ormtr_apply(int n, int m, T* z, int ldz, int nb, OrmtrWork<T> w, DescArena& arena, cudaStream_t s,
+                        const TcGemm& tc = TcGemm());
 
 // ---------------------------------------------------------------------------------------------------- two-stage
 // Stage 1 (sy2sb.cu): a (n x n, full symmetric, lda) -> band of width b in a's lower triangle and in band storage ab
@@ -186,9 +194,11 @@ cudaError_t dk_adjoint(int n, const double* c, const double* e, double mu, doubl
 // rewritten in ascending eigenvalue order.  h, s full symmetric (FP64).  work: refine_work_elems(n) doubles.
 size_t refine_work_elems(int n);
 // u (may be NULL): the upper Cholesky factor of s (ld ldu); with it C^T S C is formed as (U C)^T (U C).
+// tc (may be NULL): with a tensor-core engine, each step's update C (I + E) runs as C D (the clusters' blocks, FP64)
+// + C F (the first-order remainder, on the tensor cores).
 cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s, int lds, const double* u, int ldu,
                                double* c, int ldc, double* w, int iters, double* work, DescArena& arena,
-                               cudaStream_t st);
+                               cudaStream_t st, const TcGemm* tc = nullptr);
 
 // ---------------------------------------------------------------------------------------------------- helpers
 // Stage nprob descriptors through the arena (tile grid and tile_begin filled in from M, N) and launch one grouped GEMM.

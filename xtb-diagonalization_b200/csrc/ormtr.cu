@@ -59,9 +59,9 @@ OrmtrWork<T> ormtr_carve(T* base, int n, int m, int nb) {
 }
 
 template <typename T>
-cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, int ldz, int nb, OrmtrWork<T> w,
-                        DescArena& arena, cudaStream_t s, const TcGemm& tc) {
-  if (n <= 1 || m <= 0) return cudaSuccess;
+cudaError_t ormtr_prepare(int n, const T* a, int lda, const T* tau, int nb, OrmtrWork<T> w, DescArena& arena,
+                          cudaStream_t s, const TcGemm& tc) {
+  if (n <= 1) return cudaSuccess;
   const int nm1 = n - 1;
   const int nblocks = (nm1 + nb - 1) / nb;
   {
@@ -93,6 +93,16 @@ cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, i
   err = gemm_run(arena, tc, probs, nblocks, s);
   delete[] probs;
   if (err != cudaSuccess) return err;
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t ormtr_apply(int n, int m, T* z, int ldz, int nb, OrmtrWork<T> w, DescArena& arena, cudaStream_t s,
+                        const TcGemm& tc) {
+  if (n <= 1 || m <= 0) return cudaSuccess;
+  const int nm1 = n - 1;
+  const int nblocks = (nm1 + nb - 1) / nb;
+  cudaError_t err = cudaSuccess;
   // Apply the blocks in increasing order.  W = V_b^T Z has only kb (<= nb) rows, so its long K (the block's rows) is
   // split across slices computed in one grouped launch and summed in slice order.
   T* parts = w.W + (size_t)nb * m;
@@ -127,6 +137,15 @@ cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, i
   return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t ormtr_upper(int n, int m, const T* a, int lda, const T* tau, T* z, int ldz, int nb, OrmtrWork<T> w,
+                        DescArena& arena, cudaStream_t s, const TcGemm& tc) {
+  if (n <= 1 || m <= 0) return cudaSuccess;
+  cudaError_t err = ormtr_prepare<T>(n, a, lda, tau, nb, w, arena, s, tc);
+  if (err != cudaSuccess) return err;
+  return ormtr_apply<T>(n, m, z, ldz, nb, w, arena, s, tc);
+}
+
 template size_t ormtr_work_elems<double>(int, int, int);
 template size_t ormtr_work_elems<float>(int, int, int);
 template OrmtrWork<double> ormtr_carve<double>(double*, int, int, int);
@@ -135,5 +154,13 @@ template cudaError_t ormtr_upper<double>(int, int, const double*, int, const dou
                                          OrmtrWork<double>, DescArena&, cudaStream_t, const TcGemm&);
 template cudaError_t ormtr_upper<float>(int, int, const float*, int, const float*, float*, int, int,
                                         OrmtrWork<float>, DescArena&, cudaStream_t, const TcGemm&);
+template cudaError_t ormtr_prepare<double>(int, const double*, int, const double*, int, OrmtrWork<double>,
+                                           DescArena&, cudaStream_t, const TcGemm&);
+template cudaError_t ormtr_prepare<float>(int, const float*, int, const float*, int, OrmtrWork<float>, DescArena&,
+                                          cudaStream_t, const TcGemm&);
+template cudaError_t ormtr_apply<double>(int, int, double*, int, int, OrmtrWork<double>, DescArena&, cudaStream_t,
+                                         const TcGemm&);
+template cudaError_t ormtr_apply<float>(int, int, float*, int, int, OrmtrWork<float>, DescArena&, cudaStream_t,
+                                        const TcGemm&);
 
 }  // namespace xtbeig
