@@ -266,6 +266,55 @@ __global__ void __launch_bounds__(128) oa_cluster_kernel(int n, const double* __
   }
 }
 
+// The cluster of every index, by the runs of oa_cluster_kernel: cstart[i] = first index of i's cluster, clen[i] = its
+// length (1 for an index in no cluster).
+__global__ void oa_cluster_index_kernel(int n, const double* __restrict__ lam, const unsigned long long* dmax_bits,
+                                        int* cstart, int* clen) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double delta = oa_delta(dmax_bits);
+  auto linked = [&](int q) { return q > 0 && fabs(lam[q] - lam[q - 1]) <= delta; };
+  int s = i;
+  while (s > 0 && linked(s)) --s;
+  const int c0 = s + ((i - s) / kMaxCluster) * kMaxCluster;
+  int k = 1;
+  while (c0 + k < n && k < kMaxCluster && linked(c0 + k)) ++k;
+  cstart[i] = c0;
+  clen[i] = k;
+}
+
+// M = D + F with D the clusters' diagonal blocks of M (the identity outside clusters) and F the rest, which holds only
+// first-order corrections (about the size of the current error); F is written in FP32 for the tensor-core product.
+__global__ void oa_split_kernel(int n, const double* __restrict__ M, int ldm, const int* __restrict__ cstart,
+                                const int* __restrict__ clen, float* __restrict__ F) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= n) return;
+  const bool same = clen[j] > 1 && cstart[i] == cstart[j];
+  const double v = same ? 0.0 : M[i + (size_t)j * ldm] - (i == j ? 1.0 : 0.0);
+  F[i + (size_t)j * n] = (float)v;
+}
+
+// nxt = C D + C F = C + C (D - I) + P, with P = C F from the tensor cores: the block-diagonal part in FP64 (a column of
+// a cluster sums over its block), the small remainder from P.
+__global__ void oa_combine_kernel(int n, const double* __restrict__ C, int ldc, const double* __restrict__ M, int ldm,
+                                  const int* __restrict__ cstart, const int* __restrict__ clen,
+                                  const float* __restrict__ P, double* __restrict__ nxt, int ldn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= n) return;
+  double acc = C[i + (size_t)j * ldc];
+  const int len = clen[j];
+  if (len > 1) {
+    const int c0 = cstart[j];
+    double add = 0.0;
+    for (int q = 0; q < len; ++q)
+      add = fma(C[i + (size_t)(c0 + q) * ldc], M[(c0 + q) + (size_t)j * ldm] - (c0 + q == j ? 1.0 : 0.0), add);
+    acc += add;
+  }
+  nxt[i + (size_t)j * ldn] = acc + (double)P[i + (size_t)j * n];
+}
+
 // rank[i] = position of lam[i] in ascending order (ties by index).
 __global__ void rank_kernel(int n, const double* __restrict__ lam, int* rank) {
   __shared__ int red[32];
@@ -292,11 +341,13 @@ __global__ void scatter_columns_kernel(int n, const double* __restrict__ src, in
 
 }  // namespace
 
-size_t refine_work_elems(int n) { return (size_t)7 * n * n + 3 * (size_t)n + 64; }
+// 7 n^2 doubles (iterates, products, A, B, M), eigenvalue and index vectors, then three n^2 FP32 arrays (C, F, C F)
+// for the tensor-core update.
+size_t refine_work_elems(int n) { return (size_t)7 * n * n + 6 * (size_t)n + 160 + ((size_t)3 * n * n + 1) / 2; }
 
 cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s, int lds, const double* u, int ldu,
                                double* c, int ldc, double* w, int iters, double* work, DescArena& arena,
-                               cudaStream_t st) {
+                               cudaStream_t st, const TcGemm* tc) {
   if (n <= 0) return cudaSuccess;
   const size_t nn = (size_t)n * n;
   double* c2 = work;
@@ -310,6 +361,12 @@ cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s,
   double* lam2 = lam + n;
   int* rank = reinterpret_cast<int*>(lam2 + n);
   unsigned long long* dmax = reinterpret_cast<unsigned long long*>(lam2 + 2 * (size_t)n + 8);
+  int* cstart = reinterpret_cast<int*>(lam2 + 2 * (size_t)n + 16);
+  int* clen = cstart + n;
+  float* f32 = reinterpret_cast<float*>(lam2 + 3 * (size_t)n + 96);  // F, then C, then P = C F
+  float* c32 = f32 + nn;
+  float* p32 = c32 + nn;
+  const bool tc_update = tc && tc->passes > 0;
   // The current iterate alternates between cur and nxt; the result is scattered into c in ascending order.
   const double* cur = c;
   int ldcur = ldc;
@@ -335,8 +392,21 @@ cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s,
     oa_build_m_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(n, A, n, B, n, lam, dmax, M, n);
     oa_cluster_kernel<<<n, 128, 0, st>>>(n, A, n, B, n, lam, dmax, M, n, lam2);
     note_launches(3);
-    p[0] = gemm_problem<double>(n, n, n, 1.0, cur, ldcur, 0, M, n, 0, 0.0, nxt, n);
-    if ((err = gemm_group<double>(arena, p, 1, st)) != cudaSuccess) return err;
+    if (!tc_update) {
+      p[0] = gemm_problem<double>(n, n, n, 1.0, cur, ldcur, 0, M, n, 0, 0.0, nxt, n);
+      if ((err = gemm_group<double>(arena, p, 1, st)) != cudaSuccess) return err;
+    } else {
+      // nxt = C M = C D + C F: the clusters' rotations in FP64, the small first-order remainder F on the tensor
+      // cores (its FP32-level relative error is far below what the next step corrects).
+      oa_cluster_index_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, lam, dmax, cstart, clen);
+      oa_split_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(n, M, n, cstart, clen, f32);
+      convert_mat_f64_to_f32(n, n, cur, ldcur, c32, n, st);
+      note_launches(2);
+      GemmDesc<float> q = gemm_problem<float>(n, n, n, 1.f, c32, n, 0, f32, n, 0, 0.f, p32, n);
+      if ((err = gemm_run(arena, *tc, &q, 1, st)) != cudaSuccess) return err;
+      oa_combine_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(n, cur, ldcur, M, n, cstart, clen, p32, nxt, n);
+      note_launches();
+    }
     // next iterate: nxt; the other of c2, c3 becomes the next target (c itself is rewritten only at the end)
     cur = nxt;
     ldcur = n;
