@@ -194,8 +194,8 @@ cudaError_t dk_adjoint(int n, const double* c, const double* e, double mu, doubl
 // rewritten in ascending eigenvalue order.  h, s full symmetric (FP64).  work: refine_work_elems(n) doubles.
 size_t refine_work_elems(int n);
 // u (may be NULL): the upper Cholesky factor of s (ld ldu); with it C^T S C is formed as (U C)^T (U C).
-// tc (may be NULL): with a tensor-core engine, each step's update C (I + E) runs as C D (the clusters' blocks, FP64)
-// + C F (the first-order remainder, on the tensor cores).
+// tc (may be NULL): with a tensor-core engine, every step's update C (I + E) but the last runs as C D (the clusters'
+// blocks, FP64) + C F (the first-order remainder, on the tensor cores); the last update stays FP64.
 cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s, int lds, const double* u, int ldu,
                                double* c, int ldc, double* w, int iters, double* work, DescArena& arena,
                                cudaStream_t st, const TcGemm* tc = nullptr);

@@ -392,12 +392,14 @@ cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s,
     oa_build_m_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(n, A, n, B, n, lam, dmax, M, n);
     oa_cluster_kernel<<<n, 128, 0, st>>>(n, A, n, B, n, lam, dmax, M, n, lam2);
     note_launches(3);
-    if (!tc_update) {
+    // The tensor-core update only where a later step corrects its error (about 2e-5 relative to the correction, from
+    // the tensor cores' FP32 accumulation); the last step's update stays FP64, which sets the final accuracy.
+    if (!tc_update || it == iters - 1) {
       p[0] = gemm_problem<double>(n, n, n, 1.0, cur, ldcur, 0, M, n, 0, 0.0, nxt, n);
       if ((err = gemm_group<double>(arena, p, 1, st)) != cudaSuccess) return err;
     } else {
       // nxt = C M = C D + C F: the clusters' rotations in FP64, the small first-order remainder F on the tensor
-      // cores (its FP32-level relative error is far below what the next step corrects).
+      // cores.
       oa_cluster_index_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, lam, dmax, cstart, clen);
       oa_split_kernel<<<dim3((n + 255) / 256, n), 256, 0, st>>>(n, M, n, cstart, clen, f32);
       convert_mat_f64_to_f32(n, n, cur, ldcur, c32, n, st);
