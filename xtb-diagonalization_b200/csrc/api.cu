@@ -38,6 +38,7 @@ std::atomic<long> g_mixed_gemm{3};    // FP32 GEMMs of the mixed solve: 0 CUDA c
 std::atomic<long> g_reduction{1};     // 1: one-stage resident sytrd + ormtr; 2: two-stage sy2sb + sb2st
 std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (16, 32, 64)
 std::atomic<long> g_autotune{0};      // 1: solves use the autotuned plan nearest their size (xtb_gpu_autotune)
+std::atomic<long> g_dgemm_engine{0};  // FP64 GEMMs of xtb_dgemm_device: 0 DMMA, 1 int8 slices on tcgen05 (Ozaki)
 
 // The tunable choices of one solve.  A solve resolves its plan once (options, or the autotuned table) and every stage
 // reads it from t_plan; the plan's signature is part of the graph-cache key, so a captured graph is never replayed
@@ -1266,7 +1267,13 @@ int xtb_dgemm_device(int transa, int transb, int m, int n, int k_, double alpha,
   if (!c0) return t_state.last_code;
   Call k(c0, (cudaStream_t)stream, true);
   GemmDesc<double> p = gemm_problem<double>(m, n, k_, alpha, a, lda, transa, b, ldb, transb, beta, c, ldc);
-  k.check(gemm_group<double>(c0->arena, &p, 1, k.s), "dgemm");
+  if (g_dgemm_engine.load() == 1) {
+    const size_t wb = ozaki_work_bytes(m, n, k_);
+    char* w = k.dev<char>("ozaki.work", wb);
+    if (k.ok()) k.check(ozaki_dgemm(p, w, wb, c0->d_status, wait_limit_ns(), k.s), "ozaki dgemm");
+  } else {
+    k.check(gemm_group<double>(c0->arena, &p, 1, k.s), "dgemm");
+  }
   DeviceStatus st{};
   return k.finish(&st);
 }
@@ -1542,6 +1549,11 @@ int xtb_gpu_set_option(const char* name, long value) {
     g_autotune = value;
     return 0;
   }
+  if (!std::strcmp(name, "dgemm_engine")) {
+    if (value != 0 && value != 1) return -2;
+    g_dgemm_engine = value;
+    return 0;
+  }
   return -1;
 }
 
@@ -1559,6 +1571,7 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "reduction")) return g_reduction;
   if (!std::strcmp(name, "band_width")) return g_band_width;
   if (!std::strcmp(name, "autotune")) return g_autotune;
+  if (!std::strcmp(name, "dgemm_engine")) return g_dgemm_engine;
   return -1;
 }
 

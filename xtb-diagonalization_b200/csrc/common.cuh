@@ -25,6 +25,21 @@ struct DeviceStatus {
   int pad;
 };
 
+// Opt a kernel in to the largest dynamic shared memory per CTA the device allows beside its static shared memory.
+// The limit is one per-function setting that every host thread shares; setting it to one launch's size would race
+// with a thread launching the same kernel with a larger size (whose launch then fails), so every launch raises it to
+// the same maximum instead.  The launch itself still states its size, which alone sets the kernel's occupancy.
+template <typename Kernel>
+inline cudaError_t allow_max_dynamic_smem(Kernel kern) {
+  int dev = 0, bytes = 0;
+  cudaFuncAttributes fa;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err == cudaSuccess) err = cudaDeviceGetAttribute(&bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (err == cudaSuccess) err = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(kern));
+  if (err != cudaSuccess) return err;
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes - (int)fa.sharedSizeBytes);
+}
+
 __device__ __forceinline__ void set_status(DeviceStatus* st, int code, int info, int where) {
   if (atomicCAS(&st->code, 0, code) == 0) {
     st->info = info;

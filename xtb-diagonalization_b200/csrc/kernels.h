@@ -84,6 +84,14 @@ cudaError_t umma_gemm_group(const GemmDesc<float>* probs, int nprob, int passes,
 // Floats of tcgen05 GEMM workspace that every GEMM of an n x n solve stage fits in.
 inline size_t tc_work_elems(int n) { return 6 * (size_t)(n + 64) * (size_t)(n + 64); }
 
+// FP64 GEMM from exact int8 tcgen05 products (ozaki.cu): op(A) split by rows and op(B) by columns into 8 power-of-two
+// scaled 7-bit slices; C = alpha op(A) op(B) + beta C with an error of the order of an FP64 GEMM's relative to the
+// rows' and columns' largest entries.  K <= 65000; `work` holds ozaki_work_bytes(M, N, K) bytes.  Sizes are read
+// on the host (no device-written descriptors).
+size_t ozaki_work_bytes(int M, int N, int K);
+cudaError_t ozaki_dgemm(const GemmDesc<double>& p, void* work, size_t work_bytes, DeviceStatus* st, uint64_t limit_ns,
+                        cudaStream_t s);
+
 struct DescArena;
 // Which engine runs a stage's GEMMs: passes 0 = the grouped GEMM (FP64 DMMA / FP32 CUDA cores); for FP32 problems
 // passes 1 or 3 = the tcgen05 engine.

@@ -80,7 +80,7 @@ cudaError_t ormtr_prepare(int n, const T* a, int lda, const T* tau, int nb, Ormt
   if (err != cudaSuccess) { delete[] probs; return err; }
   {
     const size_t smem = ((size_t)nb * nb + nb) * sizeof(T);
-    err = cudaFuncSetAttribute(wy_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    err = allow_max_dynamic_smem(wy_factor_kernel<T>);
     if (err != cudaSuccess) { delete[] probs; return err; }
     wy_factor_kernel<T><<<nblocks, 128, smem, s>>>(nm1, nb, tau, w.Tf); note_launches();
   }

@@ -418,7 +418,7 @@ bool chase_segments(int n, int b, int G, int maxcols, int* seg) {
 
 template <typename T, int BW>
 cudaError_t launch_chase(const ChaseParams<T>& p, int G, size_t smem, cudaStream_t s) {
-  cudaError_t err = cudaFuncSetAttribute(sb2st_kernel<T, BW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t err = allow_max_dynamic_smem(sb2st_kernel<T, BW>);
   if (err != cudaSuccess) return err;
   if (G > 8) {
     err = cudaFuncSetAttribute(sb2st_kernel<T, BW>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -444,7 +444,7 @@ cudaError_t launch_chase(const ChaseParams<T>& p, int G, size_t smem, cudaStream
 // Largest cluster (16, else 8, else smaller) the device can place with `smem` bytes per CTA.
 template <typename T, int BW>
 int chase_cluster_size(int want, size_t smem) {
-  if (cudaFuncSetAttribute(sb2st_kernel<T, BW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+  if (allow_max_dynamic_smem(sb2st_kernel<T, BW>) != cudaSuccess)
     return 0;
   for (int G = want; G >= 1; G = G > 8 ? 8 : G - 1) {
     if (G > 8 &&
@@ -471,10 +471,9 @@ int chase_cluster_size(int want, size_t smem) {
 template <typename T, int BW>
 cudaError_t q2_launch(int n, int b, int m, int mc, int nb, const Q2Block* db, const T* w2, T* tq, T* z, int ldz,
                       int grid, size_t smem, size_t tsmem, cudaStream_t s) {
-  cudaError_t err =
-      cudaFuncSetAttribute(q2_tfactor_kernel<T, BW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
+  cudaError_t err = allow_max_dynamic_smem(q2_tfactor_kernel<T, BW>);
   if (err != cudaSuccess) return err;
-  err = cudaFuncSetAttribute(q2_apply_kernel<T, BW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  err = allow_max_dynamic_smem(q2_apply_kernel<T, BW>);
   if (err != cudaSuccess) return err;
   q2_tfactor_kernel<T, BW><<<nb, 128, tsmem, s>>>(n, b, db, w2, tq);
   q2_apply_kernel<T, BW><<<grid, 256, smem, s>>>(n, b, m, mc, nb, db, w2, tq, z, ldz);

@@ -206,8 +206,7 @@ __global__ void band_extract_kernel(int n, int b, const T* __restrict__ a, int l
 template <typename T, int BW>
 cudaError_t launch_panel(const PanelParams<T>& pp, cudaStream_t s) {
   const size_t smem = panel_smem_bytes<T, BW>(pp.ldp);
-  cudaError_t err = cudaFuncSetAttribute(panel_qr_kernel<T, BW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+  cudaError_t err = allow_max_dynamic_smem(panel_qr_kernel<T, BW>);
   if (err != cudaSuccess) return err;
   panel_qr_kernel<T, BW><<<kPanelCluster, kPanelThreads, smem, s>>>(pp);
   note_launches();

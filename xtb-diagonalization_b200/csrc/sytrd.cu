@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
 template <typename T, int NT, int CPT>
 cudaError_t launch_one(const SytrdParams<T>& p, int G, size_t smem, cudaStream_t s) {
   auto kern = p.use_smem ? sytrd_resident_kernel<T, NT, CPT, false, true> : sytrd_resident_kernel<T, NT, CPT, false, false>;
-  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t err = allow_max_dynamic_smem(kern);
   if (err != cudaSuccess) return err;
   void* args[] = {(void*)&p};
   err = cudaLaunchCooperativeKernel((void*)kern, dim3(G), dim3(NT), args, smem, s);
@@ -292,7 +292,7 @@ cudaError_t launch_one(const SytrdParams<T>& p, int G, size_t smem, cudaStream_t
 template <int CPT>
 cudaError_t launch_upper_inplace(const SytrdParams<double>& p, int G, size_t smem, cudaStream_t s) {
   auto kern = sytrd_resident_kernel<double, 512, CPT, true>;
-  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t err = allow_max_dynamic_smem(kern);
   if (err != cudaSuccess) return err;
   void* args[] = {(void*)&p};
   err = cudaLaunchCooperativeKernel((void*)kern, dim3(G), dim3(512), args, smem, s);

@@ -104,6 +104,16 @@ __device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uin
       : "memory");
 }
 
+// D(tmem, int32) (+)= A * B^T, kind::i8 (signed 8-bit operands, exact int32 accumulate).  One thread issues.
+__device__ __forceinline__ void mma_i8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 // Arrive (once) on `bar` when every tcgen05.mma issued so far by this thread has completed.
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
@@ -141,6 +151,18 @@ __device__ __forceinline__ uint64_t desc_kmajor_sw128(uint32_t saddr) {
 __device__ __forceinline__ uint64_t desc_mnmajor_sw128_32b(uint32_t saddr, uint32_t lbo_bytes) {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16) | (32ull << 32) |
          (1ull << 46) | (1ull << 61);
+}
+
+// K-major, 64B swizzle (layout type 4): rows of 64 bytes along K, 8-row groups 512 bytes apart (stride byte offset);
+// the leading byte offset is unused (encoded as 1).  A K step inside the 64-byte row advances the start address.
+__device__ __forceinline__ uint64_t desc_kmajor_sw64(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | (32ull << 32) | (1ull << 46) | (4ull << 61);
+}
+
+// Instruction descriptor, kind::i8: D S32 (bits 4-5 = 2), A and B signed 8-bit (bits 7-9, 10-12 = 1), K-major, N >> 3
+// (bits 17-22), M >> 4 (bits 24-28).
+__host__ __device__ constexpr uint32_t idesc_i8(int m, int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
 // Instruction descriptor, kind::tf32: D FP32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2), A/B major (bits 15,
