@@ -9,8 +9,8 @@ the library's splitting step by step so that the GPU engine can also be checked 
   - 8 slices by repeated rounding to nearest (half to even): y = 128 x, a_p = rint(y), x = y - a_p (|a_p| <= 64);
   - D_d = sum_{p+q=d} A_p B_q^T for d = 2..9, exact integers (here FP64 BLAS products of integer matrices, exact while
     every partial sum stays below 2^53: 8 pairs x 64^2 x K is, for K < 2^37);
-  - acc = sum_d D_d 2^-7d accumulated from d = 9 down to 2 in FP64 (each term is exact, each addition rounds once, as
-    the device's fma with a power-of-two factor does); C = alpha 2^(e_i + f_j) acc + beta C.
+  - T = sum_{d=6..9} D_d 2^(7(9-d)) and U = sum_{d=2..5} D_d 2^(7(5-d)), integers below 2^53 (exact in FP64);
+    C = alpha 2^(e_i + f_j - 63) (U 2^28 + T) + beta C, the sum U 2^28 + T rounded once.
 
 The emulation reproduces the device result exactly when beta * C is exact (beta 0 or a power of two).
 """
@@ -39,16 +39,23 @@ def split_rows(x: np.ndarray, slices: int = SLICES):
 def gemm(opa: np.ndarray, opb: np.ndarray, alpha: float = 1.0, beta: float = 0.0, c: np.ndarray | None = None,
          slices: int = SLICES) -> np.ndarray:
     """alpha op(A) op(B) + beta C as the device engine forms it (op(A): M x K, op(B): K x N, given explicitly)."""
+    assert slices == SLICES
     a, ea = split_rows(opa, slices)
     b, eb = split_rows(np.asarray(opb, dtype=np.float64).T, slices)
     m, n = opa.shape[0], opb.shape[1]
-    acc = np.zeros((m, n))
-    for d in range(slices + 1, 1, -1):
-        dd = np.zeros((m, n))
-        for p in range(max(1, d - slices), min(slices, d - 1) + 1):
-            dd += a[p - 1] @ b[d - p - 1].T  # integer sums, exact
-        acc = acc + np.ldexp(dd, -7 * d)
-    out = alpha * np.ldexp(acc, ea[:, None] + eb[None, :])
+
+    def part(dlo):  # sum_{d=dlo..dlo+3} D_d 2^(7(dlo+3-d)), Horner in 2^7 (every step an exact integer)
+        acc = np.zeros((m, n))
+        for d in range(dlo, dlo + 4):
+            dd = np.zeros((m, n))
+            for p in range(max(1, d - slices), min(slices, d - 1) + 1):
+                dd += a[p - 1] @ b[d - p - 1].T  # integer sums, exact
+            acc = acc * 128.0 + dd
+        return acc
+
+    t, u = part(6), part(2)
+    acc = u * 2.0 ** 28 + t  # one rounding
+    out = alpha * np.ldexp(acc, ea[:, None] + eb[None, :] - 63)
     if beta != 0.0:
         out = beta * np.asarray(c, dtype=np.float64) + out
     return out

@@ -5,18 +5,27 @@
 // Every row i of op(A) is scaled by a power of two 2^-ea_i (|op(A)(i,k)| < 2^(ea_i - 1)) and split into S = 8 slices
 // by repeated rounding to nearest, op(A)(i,k) = 2^ea_i (sum_p a_p(i,k) 2^-7p + r), a_p integers in [-64, 64] and
 // |r| <= 2^-57 (rounding to nearest keeps the slicing errors unbiased); every column j of op(B) likewise with 2^eb_j.
-// Then
-//   C(i,j) = 2^(ea_i + eb_j) sum_d 2^-7d D_d(i,j),   D_d = sum_{p+q=d} a_p b_q   (d = 2 .. S+1),
-// where every D_d is an exact int32 sum of int8 products (at most 8 pairs x 64^2 x K < 2^31 for K <= 65000), formed
-// by tcgen05.mma kind::i8 into its own TMEM accumulator.  Pairs with p + q > S + 1 are dropped: each is below 2^-58 of
-// the scale per product, as the slicing remainders are.  The error is therefore a small multiple of 2^-56 K times
-// the largest |op(A)| of the row times the largest |op(B)| of the column, the normwise accuracy of an FP64 GEMM.  The 36 int8 products cost 36 x 2 n^3 int8 operations,
-// which the int8 tensor pipe runs far faster than the FP64 pipe runs 2 n^3 FP64 flops.
+// With D_d = sum_{p+q=d} a_p b_q (exact int32 sums of int8 products: at most 8 pairs x 64^2 x K < 2^31 for
+// K <= 65000) the product is
+//   C(i,j) = 2^(ea_i + eb_j - 63) (U 2^28 + T),   T = sum_{d=6..9} D_d 2^(7(9-d)),   U = sum_{d=2..5} D_d 2^(7(5-d)),
+// where T and U are integers below 2^53, so both are exact in FP64 and the whole sum rounds once.  Pairs with
+// p + q > 9 are dropped: each is below 2^-58 of the scale per product, as the slicing remainders are.  The error is a
+// small multiple of 2^-56 K times the largest |op(A)| of the row times the largest |op(B)| of the column: the
+// normwise accuracy of an FP64 GEMM.  Because T and U are exact integers, the result does not depend on the order of
+// any sum: it is reproducible bit for bit.
 //
-// Pipeline per 128 x 64 output tile (128 threads): warp 0 lane 0 loads, per 64-deep K block, the 8 A slices (128 x 64
-// bytes each) and 8 B slices (64 x 64) by TMA into a 2-stage ring (64-byte swizzle); warp 1 lane 0 issues the 72
-// MMAs of the block (36 pairs x K 32 twice) into the 8 accumulators (8 x 64 = 512 TMEM columns); the four warps then
-// read the accumulators back (smallest d first), convert exactly to FP64, scale and write C.
+// Kernels (five launches per GEMM):
+//   oz_max_kernel     the largest |entry| of every row of op(A) and column of op(B) (bit patterns, atomicMax);
+//   oz_slice_kernel   the 8 int8 slices, K-contiguous [p][row][Kp], through a 64 x 64 shared-memory tile;
+//   oz_pairs_kernel   persistent; one unit = one 128 x 128 output tile and one half of the pairs: the 26 pairs with
+//                     d = 6..9 (T) or the 10 with d = 2..5 (U), each half's four D_d in four int32 TMEM accumulators
+//                     (4 x 128 = all 512 columns).  Warp 0 loads the needed slices of 32-deep K blocks by TMA into a
+//                     3-stage ring, warp 1 issues one tcgen05.mma kind::i8 (M 128, N 128, K 32) per pair and block,
+//                     eight epilogue warps turn the accumulators into T or U (exact) and store them, then free TMEM
+//                     for the next unit while warp 0 already streams that unit's blocks.
+//   oz_finish_kernel  C = alpha 2^(ea + eb - 63) fma(U, 2^28, T) + beta C.
+// An int8 MMA costs the tensor pipe a fixed ~77 cycles however small it is, so N = 128 (64 cycles of math) keeps it
+// ~83 % busy where N = 64 left it half idle; four accumulators per unit is what 512 TMEM columns allow at N = 128.
 #include <cuda.h>
 
 #include <algorithm>
@@ -29,133 +38,171 @@ namespace xtbeig {
 
 namespace {
 
-constexpr int kOzS = 8;                         // slices of 7 bits (56 >= 53)
-constexpr int kOBM = 128, kOBN = 64, kOBK = 64;  // output tile; K block (int8 elements = bytes)
-constexpr int kOStages = 2;
-constexpr int kOThreads = 128;
-constexpr int kOATile = kOBM * kOBK;             // 8 KB: one A slice of a K block
-constexpr int kOBTile = kOBN * kOBK;             // 4 KB
-constexpr int kOStageBytes = kOzS * (kOATile + kOBTile);
+constexpr int kOzS = 8;                          // slices of 7 bits (56 >= 53)
+constexpr int kOBM = 128, kOBN = 128, kOBK = 32;  // output tile; K block (int8 elements = bytes)
+constexpr int kOStages = 3;
+constexpr int kOSliceTile = kOBM * kOBK;         // 4 KB: one slice of one operand for one K block
+constexpr int kOStageBytes = 2 * kOzS * kOSliceTile;  // 64 KB: 8 A slices then 8 B slices
 constexpr int kOSmemBytes = kOStages * kOStageBytes + 1024;
-constexpr uint32_t kOTmemCols = 512;             // accumulators d = 2 .. 9, 64 columns each
+constexpr int kOEpiWarps = 8;                    // two per TMEM lane quarter, each half of the 128 columns
+constexpr int kOThreads = 32 * (2 + kOEpiWarps);
+constexpr uint32_t kOTmemCols = 512;             // four accumulators of 128 columns
 constexpr int kOzMaxK = 65000;                   // int32 exactness bound of the accumulators
 constexpr int kOzNonFinite = 1 << 20;            // exponent of a row (column) holding an Inf or a NaN
+constexpr int kOTile = 64;                       // rows x K of the slicing kernels' shared-memory tile
 
 // An operand seen as R rows of K elements: element (r, k) at X[r sr + k sk]; keep 1: only k >= r, 2: only k <= r.
 struct OzOperand {
   const double* X;
   long long sr, sk;
-  int R, K, Kp;
-  int keep;
-  unsigned long long* maxbits;  // R: bit patterns of the rows' largest |x|
-  int* e;                       // R: row exponents
+  int R, keep;
+  unsigned long long* maxbits;  // R: bit patterns of the rows' largest |x| (a NaN counts as an Inf)
   int8_t* slices;               // S x R x Kp
 };
 
+struct OzPrep {
+  OzOperand op[2];  // op(A) by rows, op(B)^T by rows (the columns of op(B))
+  int K, Kp;
+};
+
 struct OzParams {
-  CUtensorMap a, b;  // A slices [S*M rows][Kp], B slices [S*N rows][Kp], int8, K contiguous
-  const int* ea;
-  const int* eb;
-  double* C;
-  int ldc;
+  CUtensorMap a, b;  // A slices [S*M rows][Kp], B slices [S*N rows][Kp], int8, K contiguous, 32-byte swizzle
+  double* T;         // M x N (ld M): the exact high part, pairs d = 6..9
+  double* U;         // M x N (ld M): the exact low part, pairs d = 2..5
   int M, N, K;
-  double alpha, beta;
   int mode;
-  int tiles_m;
+  int tiles_m, tiles;
   DeviceStatus* st;
   unsigned long long limit_ns;
 };
 
-__device__ __forceinline__ bool oz_keep(const OzOperand& o, int r, int k) {
-  return o.keep == 0 || (o.keep == 1 ? k >= r : k <= r);
+struct OzFinish {
+  const double* T;
+  const double* U;
+  const unsigned long long* maxa;
+  const unsigned long long* maxb;
+  double* C;
+  int ldc, M, N, mode, have_k;
+  double alpha, beta;
+};
+
+__device__ __forceinline__ bool oz_keep(int keep, int r, int k) {
+  return keep == 0 || (keep == 1 ? k >= r : k <= r);
 }
 
-// Largest |x| of every row, by 32 x 32 tiles read along the stored contiguous dimension.
-__global__ void oz_rowmax_kernel(OzOperand o) {
-  __shared__ double t[32][33];
-  const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
-  const bool rc = o.sr == 1;  // rows contiguous in memory: threadIdx.x runs along r
-  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
-    const int r = r0 + (rc ? threadIdx.x : y), k = k0 + (rc ? y : threadIdx.x);
-    double v = 0.0;
-    if (r < o.R && k < o.K && oz_keep(o, r, k)) {
-      const double x = o.X[(long long)r * o.sr + (long long)k * o.sk];
-      v = isnan(x) ? __longlong_as_double(0x7ff0000000000000ll) : fabs(x);  // a NaN counts as an Inf (fmax drops NaNs)
-    }
-    if (rc) t[threadIdx.x][y] = v; else t[y][threadIdx.x] = v;
-  }
-  __syncthreads();
-  if (threadIdx.y == 0) {
-    const int r = r0 + threadIdx.x;
-    double m = 0.0;
-    for (int j = 0; j < 32; ++j) m = fmax(m, t[threadIdx.x][j]);
-    if (r < o.R && m > 0.0) atomicMax(&o.maxbits[r], (unsigned long long)__double_as_longlong(m));
-  }
-}
-
-__global__ void oz_exponent_kernel(OzOperand o) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= o.R) return;
-  const double m = __longlong_as_double((long long)o.maxbits[r]);
+// The row's scale exponent: |x| 2^-e < 1/2 for every entry; kOzNonFinite for a row holding an Inf or a NaN.
+__device__ __forceinline__ int oz_exponent(unsigned long long bits) {
+  const double m = __longlong_as_double((long long)bits);
+  if (!isfinite(m)) return kOzNonFinite;
   int e = 0;
-  if (!isfinite(m)) e = kOzNonFinite;  // the row holds an Inf or a NaN: its products are NaN
-  else if (m > 0.0) frexp(m, &e);      // m = f 2^e, f in [0.5, 1): every |x| of the row is < 2^e
-  o.e[r] = e == kOzNonFinite ? e : e + 1;
+  if (m > 0.0) frexp(m, &e);  // m = f 2^e, f in [0.5, 1)
+  return e + 1;
 }
 
-// The S slices of 32 rows x 64 K of the operand (K padded to Kp with zeros), written K-contiguous.
-__global__ void oz_slice_kernel(OzOperand o) {
-  __shared__ double t[32][65];
-  const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
-  const int tid = threadIdx.x;  // 256 threads
+// Stage the operand's 64 x 64 tile at (r0, k0) into t[row][k] (zeros outside the matrix and the kept triangle),
+// reading along whichever dimension is contiguous in memory.
+__device__ __forceinline__ void oz_load_tile(const OzOperand& o, int K, int r0, int k0, double (*t)[kOTile + 1]) {
   const bool rc = o.sr == 1;
-  for (int idx = tid; idx < 32 * 64; idx += 256) {
-    int rr, kk;
-    if (rc) { rr = idx % 32; kk = idx / 32; } else { kk = idx % 64; rr = idx / 64; }
+  for (int idx = threadIdx.x; idx < kOTile * kOTile; idx += blockDim.x) {
+    const int a = idx % kOTile, b = idx / kOTile;
+    const int rr = rc ? a : b, kk = rc ? b : a;
     const int r = r0 + rr, k = k0 + kk;
     double v = 0.0;
-    if (r < o.R && k < o.K && oz_keep(o, r, k)) v = o.X[(long long)r * o.sr + (long long)k * o.sk];
+    if (r < o.R && k < K && oz_keep(o.keep, r, k)) v = o.X[(long long)r * o.sr + (long long)k * o.sk];
     t[rr][kk] = v;
   }
+}
+
+__global__ void __launch_bounds__(256) oz_max_kernel(const __grid_constant__ OzPrep P) {
+  __shared__ double t[kOTile][kOTile + 1];
+  const OzOperand& o = P.op[blockIdx.z];
+  const int r0 = blockIdx.x * kOTile, k0 = blockIdx.y * kOTile;
+  if (r0 >= o.R) return;
+  oz_load_tile(o, P.K, r0, k0, t);
   __syncthreads();
-  const size_t plane = (size_t)o.R * o.Kp;
-  for (int idx = tid; idx < 32 * 64; idx += 256) {
-    const int kk = idx % 64, rr = idx / 64;
-    const int r = r0 + rr, k = k0 + kk;
-    if (r >= o.R || k >= o.Kp) continue;
-    const int e = o.e[r];
-    double x = e == kOzNonFinite ? 0.0 : ldexp(t[rr][kk], -e);  // |x| < 1/2, exact
-    int8_t* dst = o.slices + (size_t)r * o.Kp + k;
+  // 4 threads per row, 16 entries each, then a 4-lane max.
+  const int rr = threadIdx.x >> 2, part = threadIdx.x & 3;
+  double m = 0.0;
 #pragma unroll
-    for (int p = 0; p < kOzS; ++p) {
-      const double y = x * 128.0;  // |y| <= 64
-      const double a = rint(y);    // |a| <= 64
-      x = y - a;                   // exact, |x| <= 1/2
-      dst[(size_t)p * plane] = (int8_t)(int)a;
+  for (int j = 0; j < kOTile / 4; ++j) {
+    const double x = t[rr][part * (kOTile / 4) + j];
+    m = fmax(m, isnan(x) ? __longlong_as_double(0x7ff0000000000000ll) : fabs(x));  // a NaN counts as an Inf
+  }
+  m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 1));
+  m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 2));
+  if (part == 0 && r0 + rr < o.R && m > 0.0)
+    atomicMax(&o.maxbits[r0 + rr], (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void __launch_bounds__(256) oz_slice_kernel(const __grid_constant__ OzPrep P) {
+  __shared__ double t[kOTile][kOTile + 1];
+  const OzOperand& o = P.op[blockIdx.z];
+  const int r0 = blockIdx.x * kOTile, k0 = blockIdx.y * kOTile;
+  if (r0 >= o.R) return;
+  oz_load_tile(o, P.K, r0, k0, t);
+  __syncthreads();
+  const size_t plane = (size_t)o.R * P.Kp;
+  // Work item: one row, 8 consecutive K; its 8 slices are written as one 8-byte word each (8 lanes cover a row's 64
+  // bytes).
+  for (int item = threadIdx.x; item < kOTile * (kOTile / 8); item += blockDim.x) {
+    const int g = item & 7, rr = item >> 3;
+    const int r = r0 + rr, k = k0 + g * 8;
+    if (r >= o.R || k >= P.Kp) continue;
+    const int e = oz_exponent(o.maxbits[r]);
+    unsigned long long word[kOzS];
+#pragma unroll
+    for (int p = 0; p < kOzS; ++p) word[p] = 0ull;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      double x = e == kOzNonFinite ? 0.0 : ldexp(t[rr][g * 8 + j], -e);  // |x| < 1/2, exact
+#pragma unroll
+      for (int p = 0; p < kOzS; ++p) {
+        const double y = x * 128.0;  // |y| <= 64
+        const double a = rint(y);    // |a| <= 64
+        x = y - a;                   // exact, |x| <= 1/2
+        word[p] |= (unsigned long long)(uint8_t)(int8_t)(int)a << (8 * j);
+      }
     }
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(o.slices + (size_t)r * P.Kp + k);
+#pragma unroll
+    for (int p = 0; p < kOzS; ++p) dst[(size_t)p * plane / 8] = word[p];
   }
 }
 
-__global__ void __launch_bounds__(kOThreads, 1) ozaki_gemm_kernel(const __grid_constant__ OzParams P) {
+// Unit u of the persistent schedule: u < tiles the T half of tile u, else the U half of tile u - tiles.  Returns false
+// for a tile that kCUpper skips.  kb0 / nk: the K blocks the tile's triangular operands leave nonzero.
+struct OzUnit {
+  int m0, n0, kb0, nk, high;
+};
+__device__ __forceinline__ bool oz_unit(const OzParams& P, int u, OzUnit& w) {
+  const int tile = u < P.tiles ? u : u - P.tiles;
+  w.high = u < P.tiles;
+  w.m0 = (tile % P.tiles_m) * kOBM;
+  w.n0 = (tile / P.tiles_m) * kOBN;
+  if ((P.mode & kCUpper) && w.m0 >= w.n0 + kOBN) return false;
+  int kbeg = 0, kend = P.K;
+  if (P.mode & kTriAUpper) kbeg = max(kbeg, w.m0);
+  if (P.mode & kTriALower) kend = min(kend, w.m0 + kOBM);
+  if (P.mode & kTriBUpper) kend = min(kend, w.n0 + kOBN);
+  if (P.mode & kTriBLower) kbeg = max(kbeg, w.n0);
+  w.kb0 = kbeg / kOBK;
+  w.nk = kend > kbeg ? (kend + kOBK - 1) / kOBK - w.kb0 : 0;
+  return true;
+}
+
+__global__ void __launch_bounds__(kOThreads, 1) oz_pairs_kernel(const __grid_constant__ OzParams P) {
   extern __shared__ unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kOStages];
   __shared__ __align__(8) uint64_t empty_bar[kOStages];
-  __shared__ __align__(8) uint64_t done_bar;
+  __shared__ __align__(8) uint64_t done_bar;   // the unit's MMAs have completed
+  __shared__ __align__(8) uint64_t free_bar;   // the epilogue has read the unit's accumulators
   __shared__ uint32_t tmem_base;
   __shared__ volatile int s_abort;
 
   unsigned char* smem =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = (blockIdx.x % P.tiles_m) * kOBM, n0 = (blockIdx.x / P.tiles_m) * kOBN;
-  if ((P.mode & kCUpper) && m0 >= n0 + kOBN) return;
-  int kbeg = 0, kend = P.K;
-  if (P.mode & kTriAUpper) kbeg = max(kbeg, m0);
-  if (P.mode & kTriALower) kend = min(kend, m0 + kOBM);
-  if (P.mode & kTriBUpper) kend = min(kend, n0 + kOBN);
-  if (P.mode & kTriBLower) kbeg = max(kbeg, n0);
-  const int kb0 = kbeg / kOBK;
-  const int nk = kend > kbeg ? (kend + kOBK - 1) / kOBK - kb0 : 0;
+  const int nunits = 2 * P.tiles;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kOStages; ++s) {
@@ -163,6 +210,7 @@ __global__ void __launch_bounds__(kOThreads, 1) ozaki_gemm_kernel(const __grid_c
       umma::mbar_init(&empty_bar[s], 1);
     }
     umma::mbar_init(&done_bar, 1);
+    umma::mbar_init(&free_bar, kOEpiWarps);
     umma::fence_barrier_init();
     s_abort = 0;
   }
@@ -172,99 +220,148 @@ __global__ void __launch_bounds__(kOThreads, 1) ozaki_gemm_kernel(const __grid_c
   umma::tc_fence_after();
   const uint32_t tmem = tmem_base;
 
-  if (nk > 0 && warp == 0 && lane == 0) {
-    umma::prefetch_tensormap(&P.a);
-    umma::prefetch_tensormap(&P.b);
-    for (int i = 0; i < nk; ++i) {
-      const int s = i % kOStages;
-      if (i >= kOStages && !umma::mbar_wait(&empty_bar[s], ((i / kOStages) - 1) & 1, P.limit_ns)) {
-        set_status(P.st, kStatusBarrierTimeout, 0, 11);
-        s_abort = 1;
-        break;
+  if (warp == 0) {
+    if (lane == 0) {
+      umma::prefetch_tensormap(&P.a);
+      umma::prefetch_tensormap(&P.b);
+      uint32_t it = 0;  // K blocks loaded so far (ring position)
+      for (int u = blockIdx.x; u < nunits && !s_abort; u += gridDim.x) {
+        OzUnit w;
+        if (!oz_unit(P, u, w)) continue;
+        const int ns = w.high ? kOzS : 4;  // slices the unit's pairs use
+        for (int i = 0; i < w.nk; ++i, ++it) {
+          const int s = it % kOStages;
+          if (it >= kOStages && !umma::mbar_wait(&empty_bar[s], ((it / kOStages) - 1) & 1, P.limit_ns)) {
+            set_status(P.st, kStatusBarrierTimeout, 0, 21);
+            s_abort = 1;
+            break;
+          }
+          if (s_abort) break;
+          unsigned char* st = smem + (size_t)s * kOStageBytes;
+          const int k0 = (w.kb0 + i) * kOBK;
+          umma::mbar_arrive_expect_tx(&full_bar[s], (uint32_t)(2 * ns * kOSliceTile));
+          for (int p = 0; p < ns; ++p)
+            umma::tma_load_2d(st + p * kOSliceTile, &P.a, &full_bar[s], k0, p * P.M + w.m0);
+          for (int q = 0; q < ns; ++q)
+            umma::tma_load_2d(st + (kOzS + q) * kOSliceTile, &P.b, &full_bar[s], k0, q * P.N + w.n0);
+        }
       }
-      if (s_abort) break;
-      unsigned char* st = smem + (size_t)s * kOStageBytes;
-      const int k0 = (kb0 + i) * kOBK;
-      umma::mbar_arrive_expect_tx(&full_bar[s], (uint32_t)kOStageBytes);
-      for (int p = 0; p < kOzS; ++p) umma::tma_load_2d(st + p * kOATile, &P.a, &full_bar[s], k0, p * P.M + m0);
-      for (int q = 0; q < kOzS; ++q)
-        umma::tma_load_2d(st + kOzS * kOATile + q * kOBTile, &P.b, &full_bar[s], k0, q * P.N + n0);
     }
-  } else if (nk > 0 && warp == 1 && lane == 0) {
-    const uint32_t idesc = umma::idesc_i8(kOBM, kOBN);
-    for (int i = 0; i < nk; ++i) {
-      const int s = i % kOStages;
-      if (!umma::mbar_wait(&full_bar[s], (i / kOStages) & 1, P.limit_ns)) {
-        set_status(P.st, kStatusBarrierTimeout, 0, 12);
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = umma::idesc_i8(kOBM, kOBN);
+      uint32_t it = 0, nu = 0;
+      for (int u = blockIdx.x; u < nunits && !s_abort; u += gridDim.x) {
+        OzUnit w;
+        if (!oz_unit(P, u, w)) continue;
+        if (nu > 0 && !umma::mbar_wait(&free_bar, (nu - 1) & 1, P.limit_ns)) {
+          set_status(P.st, kStatusBarrierTimeout, 0, 22);
+          s_abort = 1;
+          break;
+        }
+        umma::tc_fence_after();
+        const int dlo = w.high ? 6 : 2;
+        for (int i = 0; i < w.nk; ++i, ++it) {
+          const int s = it % kOStages;
+          if (!umma::mbar_wait(&full_bar[s], (it / kOStages) & 1, P.limit_ns)) {
+            set_status(P.st, kStatusBarrierTimeout, 0, 23);
+            s_abort = 1;
+            break;
+          }
+          if (s_abort) break;
+          umma::tc_fence_after();
+          const uint32_t sa = umma::smem_addr(smem + (size_t)s * kOStageBytes);
+          const uint32_t sb = sa + kOzS * kOSliceTile;
+          for (int d = dlo; d < dlo + 4; ++d) {
+            const int p_lo = max(1, d - kOzS), p_hi = min(kOzS, d - 1);
+            for (int p = p_lo; p <= p_hi; ++p) {
+              const uint64_t ad = umma::desc_kmajor_sw32(sa + (p - 1) * kOSliceTile);
+              const uint64_t bd = umma::desc_kmajor_sw32(sb + (d - p - 1) * kOSliceTile);
+              umma::mma_i8(tmem + (uint32_t)(d - dlo) * kOBN, ad, bd, idesc, (i == 0 && p == p_lo) ? 0u : 1u);
+            }
+          }
+          umma::mma_commit(&empty_bar[s]);
+        }
+        if (s_abort) break;
+        umma::mma_commit(&done_bar);
+        ++nu;
+      }
+    }
+  } else {
+    // Epilogue warps 2..9: TMEM lane quarter warp % 4 (the rows), column half (warp - 2) / 4.
+    const int quarter = warp & 3, half = (warp - 2) >> 2;
+    uint32_t nu = 0;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+      OzUnit w;
+      if (!oz_unit(P, u, w)) continue;
+      const bool ok = __all_sync(0xffffffffu, umma::mbar_wait(&done_bar, nu & 1, P.limit_ns) ? 1 : 0) != 0;
+      if (!ok) {
+        if (lane == 0) set_status(P.st, kStatusBarrierTimeout, 0, 24);
         s_abort = 1;
         break;
       }
-      if (s_abort) break;
       umma::tc_fence_after();
-      const uint32_t sa = umma::smem_addr(smem + (size_t)s * kOStageBytes);
-      const uint32_t sb = sa + kOzS * kOATile;
-      for (int d = 2; d <= kOzS + 1; ++d) {
-        const int p_lo = max(1, d - kOzS), p_hi = min(kOzS, d - 1);
-        for (int p = p_lo; p <= p_hi; ++p) {
-          const int q = d - p;
+      const int row = w.m0 + quarter * 32 + lane;
+      double* out = w.high ? P.T : P.U;
+      for (int c = half * 64; c < half * 64 + 64; c += 32) {
+        double acc[32];
+        if (w.nk > 0) {
+          uint32_t r[32];
+          const uint32_t base = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c;
+          umma::tmem_ld32(base, r);
 #pragma unroll
-          for (int kk = 0; kk < kOBK / 32; ++kk) {
-            const uint64_t ad = umma::desc_kmajor_sw64(sa + (p - 1) * kOATile + kk * 32);
-            const uint64_t bd = umma::desc_kmajor_sw64(sb + (q - 1) * kOBTile + kk * 32);
-            const bool first = i == 0 && p == p_lo && kk == 0;
-            umma::mma_i8(tmem + (uint32_t)(d - 2) * kOBN, ad, bd, idesc, first ? 0u : 1u);
+          for (int j = 0; j < 32; ++j) acc[j] = (double)(int)r[j];
+#pragma unroll
+          for (int a = 1; a < 4; ++a) {  // Horner in 2^7, exact: every partial sum is an integer below 2^53
+            umma::tmem_ld32(base + (uint32_t)(a * kOBN), r);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) acc[j] = fma(acc[j], 128.0, (double)(int)r[j]);
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+        }
+        if (row < P.M) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int col = w.n0 + c + j;
+            if (col < P.N) out[row + (size_t)col * P.M] = acc[j];
           }
         }
       }
-      umma::mma_commit(&empty_bar[s]);
+      umma::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) umma::mbar_arrive(&free_bar);
+      ++nu;
     }
-    umma::mma_commit(&done_bar);
   }
-  __syncwarp();
 
-  bool have = nk > 0;
-  if (have) {
-    have = __all_sync(0xffffffffu, umma::mbar_wait(&done_bar, 0, P.limit_ns) ? 1 : 0) != 0;
-    if (!have && lane == 0) set_status(P.st, kStatusBarrierTimeout, 0, 13);
-    umma::tc_fence_after();
-  }
-  __syncwarp();
-  const int row = m0 + warp * 32 + lane;
-  const int ea = row < P.M ? P.ea[row] : 0;
-  const double alpha = P.alpha, beta = P.beta;
-  for (int c = 0; c < kOBN; c += 32) {
-    double acc[32];
-#pragma unroll
-    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
-    if (have) {
-      for (int d = kOzS + 1; d >= 2; --d) {  // smallest terms first
-        uint32_t r[32];
-        umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d - 2) * kOBN + (uint32_t)c, r);
-        const double sc = ldexp(1.0, -7 * d);
-#pragma unroll
-        for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)r[j], sc, acc[j]);
-      }
-    }
-    if (row < P.M) {
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const int col = n0 + c + j;
-        if (col < P.N) {
-          double* cp = P.C + row + (size_t)col * P.ldc;
-          const int eb = P.eb[col];
-          double v = (ea == kOzNonFinite || eb == kOzNonFinite) ? __longlong_as_double(0x7ff8000000000000ll)
-                                                                 : alpha * ldexp(acc[j], ea + eb);
-          if (beta != 0.0) v = fma(beta, *cp, v);
-          *cp = v;
-        }
-      }
-    }
-  }
   umma::tc_fence_before();
   __syncthreads();
   if (warp == 2) {
     umma::tc_fence_after();
     umma::tmem_dealloc(tmem, kOTmemCols);
+  }
+}
+
+__global__ void oz_finish_kernel(const __grid_constant__ OzFinish F) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= F.M) return;
+  const int ea = oz_exponent(F.maxa[i]);
+  for (int j = blockIdx.y; j < F.N; j += gridDim.y) {
+    if ((F.mode & kCUpper) && (i / kOBM) * kOBM >= (j / kOBN) * kOBN + kOBN) continue;  // tiles the pairs kernel skips
+    const int eb = oz_exponent(F.maxb[j]);
+    double* cp = F.C + i + (size_t)j * F.ldc;
+    double v;
+    if (ea == kOzNonFinite || eb == kOzNonFinite) {
+      v = __longlong_as_double(0x7ff8000000000000ll);
+    } else {
+      const size_t at = i + (size_t)j * F.M;
+      const double acc = F.have_k ? fma(F.U[at], 268435456.0, F.T[at]) : 0.0;  // U 2^28 + T, one rounding
+      v = F.alpha * ldexp(acc, ea + eb - 63);
+    }
+    if (F.beta != 0.0) v = fma(F.beta, *cp, v);
+    *cp = v;
   }
 }
 
@@ -285,39 +382,30 @@ EncodeTiledFn oz_encode_fn() {
   return fn;
 }
 
-// rows x Kp int8 (rows = S x R), box 64 bytes x box_rows, 64-byte swizzle.
-bool oz_encode(CUtensorMap* map, const int8_t* base, int rows, int Kp, int box_rows) {
+// rows x Kp int8 (rows = S x R), box 32 bytes x 128 rows, 32-byte swizzle.
+bool oz_encode(CUtensorMap* map, const int8_t* base, int rows, int Kp) {
   EncodeTiledFn fn = oz_encode_fn();
   if (!fn) return false;
   cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)Kp};
-  cuuint32_t box[2] = {64u, (cuuint32_t)box_rows};
+  cuuint32_t box[2] = {(cuuint32_t)kOBK, 128u};
   cuuint32_t estr[2] = {1u, 1u};
   return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(base), dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-inline int oz_kp(int K) { return (std::max(K, 1) + 63) / 64 * 64; }
+inline int oz_kp(int K) { return (std::max(K, 1) + kOTile - 1) / kOTile * kOTile; }
 inline size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
 
 bool g_oz_smem[64];
-
-void oz_prepare(const OzOperand& o, cudaStream_t s) {
-  dim3 g1((o.R + 31) / 32, (o.K + 31) / 32);
-  oz_rowmax_kernel<<<g1, dim3(32, 8), 0, s>>>(o);
-  oz_exponent_kernel<<<(o.R + 255) / 256, 256, 0, s>>>(o);
-  dim3 g2((o.R + 31) / 32, o.Kp / 64);
-  oz_slice_kernel<<<g2, 256, 0, s>>>(o);
-  note_launches(3);
-}
 
 }  // namespace
 
 size_t ozaki_work_bytes(int M, int N, int K) {
   const size_t kp = (size_t)oz_kp(K);
-  return up256((size_t)kOzS * M * kp) + up256((size_t)kOzS * N * kp) + up256((size_t)(M + N) * 8) +
-         up256((size_t)(M + N) * 4) + 256;
+  return up256((size_t)kOzS * M * kp) + up256((size_t)kOzS * N * kp) + 2 * up256((size_t)M * N * 8) +
+         up256((size_t)(M + N) * 8) + 256;
 }
 
 cudaError_t ozaki_dgemm(const GemmDesc<double>& p, void* work, size_t work_bytes, DeviceStatus* st, uint64_t limit_ns,
@@ -331,66 +419,77 @@ cudaError_t ozaki_dgemm(const GemmDesc<double>& p, void* work, size_t work_bytes
   w += up256((size_t)kOzS * p.M * Kp);
   int8_t* sb = reinterpret_cast<int8_t*>(w);
   w += up256((size_t)kOzS * p.N * Kp);
+  double* T = reinterpret_cast<double*>(w);
+  w += up256((size_t)p.M * p.N * 8);
+  double* U = reinterpret_cast<double*>(w);
+  w += up256((size_t)p.M * p.N * 8);
   unsigned long long* maxbits = reinterpret_cast<unsigned long long*>(w);
-  w += up256((size_t)(p.M + p.N) * 8);
-  int* ex = reinterpret_cast<int*>(w);
   cudaError_t err = cudaMemsetAsync(maxbits, 0, (size_t)(p.M + p.N) * 8, s);
   if (err != cudaSuccess) return err;
   if (K > 0) {
-    OzOperand oa;
+    OzPrep P;
+    memset(&P, 0, sizeof(P));
+    OzOperand& oa = P.op[0];
     oa.X = p.A;
     oa.sr = p.transA ? p.lda : 1;
     oa.sk = p.transA ? 1 : p.lda;
     oa.R = p.M;
-    oa.K = K;
-    oa.Kp = Kp;
     oa.keep = (p.mode & kTriAUpper) ? 1 : (p.mode & kTriALower) ? 2 : 0;
     oa.maxbits = maxbits;
-    oa.e = ex;
     oa.slices = sa;
-    OzOperand ob;
+    OzOperand& ob = P.op[1];
     ob.X = p.B;  // op(B)^T: row n, element k = op(B)(k, n)
     ob.sr = p.transB ? 1 : p.ldb;
     ob.sk = p.transB ? p.ldb : 1;
     ob.R = p.N;
-    ob.K = K;
-    ob.Kp = Kp;
     ob.keep = (p.mode & kTriBUpper) ? 2 : (p.mode & kTriBLower) ? 1 : 0;
     ob.maxbits = maxbits + p.M;
-    ob.e = ex + p.M;
     ob.slices = sb;
-    oz_prepare(oa, s);
-    oz_prepare(ob, s);
-  } else {
-    err = cudaMemsetAsync(ex, 0, (size_t)(p.M + p.N) * 4, s);
-    if (err != cudaSuccess) return err;
+    P.K = K;
+    P.Kp = Kp;
+    const dim3 grid((std::max(p.M, p.N) + kOTile - 1) / kOTile, Kp / kOTile, 2);
+    oz_max_kernel<<<grid, 256, 0, s>>>(P);
+    oz_slice_kernel<<<grid, 256, 0, s>>>(P);
+    note_launches(2);
+
+    OzParams Q;
+    memset(&Q, 0, sizeof(Q));
+    if (!oz_encode(&Q.a, sa, kOzS * p.M, Kp) || !oz_encode(&Q.b, sb, kOzS * p.N, Kp)) return cudaErrorInvalidValue;
+    Q.T = T;
+    Q.U = U;
+    Q.M = p.M;
+    Q.N = p.N;
+    Q.K = K;
+    Q.mode = p.mode;
+    Q.tiles_m = (p.M + kOBM - 1) / kOBM;
+    Q.tiles = Q.tiles_m * ((p.N + kOBN - 1) / kOBN);
+    Q.st = st;
+    Q.limit_ns = limit_ns;
+    int dev = 0, sms = 0;
+    if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
+    if ((err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return err;
+    if (dev < 0 || dev >= 64 || !g_oz_smem[dev]) {
+      err = cudaFuncSetAttribute(oz_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOSmemBytes);
+      if (err != cudaSuccess) return err;
+      if (dev >= 0 && dev < 64) g_oz_smem[dev] = true;
+    }
+    oz_pairs_kernel<<<std::min(2 * Q.tiles, sms), kOThreads, kOSmemBytes, s>>>(Q);
+    note_launches();
   }
-  OzParams P;
-  memset(&P, 0, sizeof(P));
-  if (K > 0 && (!oz_encode(&P.a, sa, kOzS * p.M, Kp, kOBM) || !oz_encode(&P.b, sb, kOzS * p.N, Kp, kOBN)))
-    return cudaErrorInvalidValue;
-  P.ea = ex;
-  P.eb = ex + p.M;
-  P.C = p.C;
-  P.ldc = p.ldc;
-  P.M = p.M;
-  P.N = p.N;
-  P.K = K;
-  P.alpha = p.alpha;
-  P.beta = p.beta;
-  P.mode = p.mode;
-  P.tiles_m = (p.M + kOBM - 1) / kOBM;
-  P.st = st;
-  P.limit_ns = limit_ns;
-  const int tiles = P.tiles_m * ((p.N + kOBN - 1) / kOBN);
-  int dev = 0;
-  if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
-  if (dev < 0 || dev >= 64 || !g_oz_smem[dev]) {
-    err = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOSmemBytes);
-    if (err != cudaSuccess) return err;
-    if (dev >= 0 && dev < 64) g_oz_smem[dev] = true;
-  }
-  ozaki_gemm_kernel<<<tiles, kOThreads, kOSmemBytes, s>>>(P);
+  OzFinish F;
+  F.T = T;
+  F.U = U;
+  F.maxa = maxbits;
+  F.maxb = maxbits + p.M;
+  F.C = p.C;
+  F.ldc = p.ldc;
+  F.M = p.M;
+  F.N = p.N;
+  F.mode = p.mode;
+  F.have_k = K > 0;
+  F.alpha = p.alpha;
+  F.beta = p.beta;
+  oz_finish_kernel<<<dim3((p.M + 255) / 256, std::min(p.N, 65535)), 256, 0, s>>>(F);
   note_launches();
   return cudaGetLastError();
 }

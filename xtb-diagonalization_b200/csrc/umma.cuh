@@ -153,10 +153,11 @@ __device__ __forceinline__ uint64_t desc_mnmajor_sw128_32b(uint32_t saddr, uint3
          (1ull << 46) | (1ull << 61);
 }
 
-// K-major, 64B swizzle (layout type 4): rows of 64 bytes along K, 8-row groups 512 bytes apart (stride byte offset);
-// the leading byte offset is unused (encoded as 1).  A K step inside the 64-byte row advances the start address.
-__device__ __forceinline__ uint64_t desc_kmajor_sw64(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | (32ull << 32) | (1ull << 46) | (4ull << 61);
+// K-major, 32B swizzle (layout type 6): rows of 32 bytes along K (one K step of an 8-bit MMA), 8-row groups 256
+// bytes apart (stride byte offset); the leading byte offset is unused (encoded as 1).  TMA writes this layout with
+// CU_TENSOR_MAP_SWIZZLE_32B and a 32-byte inner box.
+__device__ __forceinline__ uint64_t desc_kmajor_sw32(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | (16ull << 32) | (1ull << 46) | (6ull << 61);
 }
 
 // Instruction descriptor, kind::i8: D S32 (bits 4-5 = 2), A and B signed 8-bit (bits 7-9, 10-12 = 1), K-major, N >> 3
