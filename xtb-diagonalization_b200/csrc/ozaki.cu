@@ -19,10 +19,10 @@
 //   oz_slice_kernel   the 8 int8 slices, K-contiguous [p][row][Kp], through a 64 x 64 shared-memory tile;
 //   oz_pairs_kernel   persistent; one unit = one 128 x 128 output tile and one half of the pairs: the 26 pairs with
 //                     d = 6..9 (T) or the 10 with d = 2..5 (U), each half's four D_d in four int32 TMEM accumulators
-//                     (4 x 128 = all 512 columns).  Warp 0 loads the needed slices of 32-deep K blocks by TMA into a
-//                     3-stage ring, warp 1 issues one tcgen05.mma kind::i8 (M 128, N 128, K 32) per pair and block,
-//                     eight epilogue warps turn the accumulators into T or U (exact) and store them, then free TMEM
-//                     for the next unit while warp 0 already streams that unit's blocks.
+//                     (4 x 128 = all 512 columns); units are taken from a global counter, heavier ones first.  Warp 0
+//                     loads the needed slices of 32-deep K blocks by TMA into a 3-stage ring, warp 1 issues one
+//                     tcgen05.mma kind::i8 (M 128, N 128, K 32) per pair and block, eight epilogue warps read the
+//                     accumulators as T or U (exact), free TMEM for the next unit's MMAs, then store.
 //   oz_finish_kernel  C = alpha 2^(ea + eb - 63) fma(U, 2^28, T) + beta C.
 // An int8 MMA costs the tensor pipe a fixed ~77 cycles however small it is, so N = 128 (64 cycles of math) keeps it
 // ~83 % busy where N = 64 left it half idle; four accumulators per unit is what 512 TMEM columns allow at N = 128.
@@ -72,6 +72,7 @@ struct OzParams {
   int M, N, K;
   int mode;
   int tiles_m, tiles;
+  unsigned* counter;  // next unit to hand out (zero at launch)
   DeviceStatus* st;
   unsigned long long limit_ns;
 };
@@ -101,15 +102,23 @@ __device__ __forceinline__ int oz_exponent(unsigned long long bits) {
 
 // Stage the operand's 64 x 64 tile at (r0, k0) into t[row][k] (zeros outside the matrix and the kept triangle),
 // reading along whichever dimension is contiguous in memory.
+// All 16 loads of a thread are issued before the first store, so they are in flight together.  256 threads.
 __device__ __forceinline__ void oz_load_tile(const OzOperand& o, int K, int r0, int k0, double (*t)[kOTile + 1]) {
+  constexpr int kPer = kOTile * kOTile / 256;
   const bool rc = o.sr == 1;
-  for (int idx = threadIdx.x; idx < kOTile * kOTile; idx += blockDim.x) {
+  double v[kPer];
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int idx = threadIdx.x + 256 * j;
     const int a = idx % kOTile, b = idx / kOTile;
-    const int rr = rc ? a : b, kk = rc ? b : a;
-    const int r = r0 + rr, k = k0 + kk;
-    double v = 0.0;
-    if (r < o.R && k < K && oz_keep(o.keep, r, k)) v = o.X[(long long)r * o.sr + (long long)k * o.sk];
-    t[rr][kk] = v;
+    const int r = r0 + (rc ? a : b), k = k0 + (rc ? b : a);
+    v[j] = (r < o.R && k < K && oz_keep(o.keep, r, k)) ? o.X[(long long)r * o.sr + (long long)k * o.sk] : 0.0;
+  }
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int idx = threadIdx.x + 256 * j;
+    const int a = idx % kOTile, b = idx / kOTile;
+    if (rc) t[a][b] = v[j]; else t[b][a] = v[j];
   }
 }
 
@@ -149,18 +158,23 @@ __global__ void __launch_bounds__(256) oz_slice_kernel(const __grid_constant__ O
     const int r = r0 + rr, k = k0 + g * 8;
     if (r >= o.R || k >= P.Kp) continue;
     const int e = oz_exponent(o.maxbits[r]);
+    const double scale = e == kOzNonFinite ? 0.0 : ldexp(1.0, -e);  // a power of two: x * scale == ldexp(x, -e)
+    // Rounding to nearest (ties to even) by the 1.5 x 2^52 shift: y + kShift holds rint(y) in its low mantissa bits
+    // (|y| <= 64), so the slice's integer is read off the low word without a conversion instruction.
+    constexpr double kShift = 6755399441055744.0;
     unsigned long long word[kOzS];
 #pragma unroll
     for (int p = 0; p < kOzS; ++p) word[p] = 0ull;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      double x = e == kOzNonFinite ? 0.0 : ldexp(t[rr][g * 8 + j], -e);  // |x| < 1/2, exact
+      double x = t[rr][g * 8 + j] * scale;  // |x| < 1/2, exact
 #pragma unroll
       for (int p = 0; p < kOzS; ++p) {
-        const double y = x * 128.0;  // |y| <= 64
-        const double a = rint(y);    // |a| <= 64
-        x = y - a;                   // exact, |x| <= 1/2
-        word[p] |= (unsigned long long)(uint8_t)(int8_t)(int)a << (8 * j);
+        const double y = x * 128.0;                 // |y| <= 64
+        const double sh = __dadd_rn(y, kShift);     // kShift + rint(y)
+        const double a = __dsub_rn(sh, kShift);     // rint(y), |a| <= 64
+        x = y - a;                                  // exact, |x| <= 1/2
+        word[p] |= (unsigned long long)(uint8_t)__double2loint(sh) << (8 * j);
       }
     }
     unsigned long long* dst = reinterpret_cast<unsigned long long*>(o.slices + (size_t)r * P.Kp + k);
@@ -190,12 +204,34 @@ __device__ __forceinline__ bool oz_unit(const OzParams& P, int u, OzUnit& w) {
   return true;
 }
 
+// The epilogue's view of one unit: the 64 columns [c0, c0 + 64) of this warp's 32 rows as exact FP64 integers,
+// Horner in 2^7 over the four accumulators (every partial sum is an integer below 2^53).
+__device__ __forceinline__ void oz_read_unit(uint32_t taddr, double (&v)[32]) {
+  uint32_t r[32];
+  umma::tmem_ld32(taddr, r);
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = (double)(int)r[j];
+#pragma unroll
+  for (int a = 1; a < 4; ++a) {
+    umma::tmem_ld32(taddr + (uint32_t)(a * kOBN), r);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = fma(v[j], 128.0, (double)(int)r[j]);
+  }
+}
+
+// Units are handed out by a global counter in the order T units, then U units (the heavier first), so the CTAs
+// balance the uneven units themselves.  Warp 0 takes a unit, streams its K blocks and tags every stage with the unit;
+// warp 1 reads the tag of a unit's first stage, tells the epilogue which unit comes next (meta_bar) and issues its
+// MMAs; a tag of -1 ends both.
 __global__ void __launch_bounds__(kOThreads, 1) oz_pairs_kernel(const __grid_constant__ OzParams P) {
   extern __shared__ unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kOStages];
   __shared__ __align__(8) uint64_t empty_bar[kOStages];
   __shared__ __align__(8) uint64_t done_bar;   // the unit's MMAs have completed
   __shared__ __align__(8) uint64_t free_bar;   // the epilogue has read the unit's accumulators
+  __shared__ __align__(8) uint64_t meta_bar;   // the next unit's id is in meta_unit[]
+  __shared__ int stage_unit[kOStages];         // the unit whose K blocks a stage holds; -1: no more units
+  __shared__ int meta_unit[2];
   __shared__ uint32_t tmem_base;
   __shared__ volatile int s_abort;
 
@@ -211,6 +247,7 @@ __global__ void __launch_bounds__(kOThreads, 1) oz_pairs_kernel(const __grid_con
     }
     umma::mbar_init(&done_bar, 1);
     umma::mbar_init(&free_bar, kOEpiWarps);
+    umma::mbar_init(&meta_bar, 1);
     umma::fence_barrier_init();
     s_abort = 0;
   }
@@ -224,12 +261,18 @@ __global__ void __launch_bounds__(kOThreads, 1) oz_pairs_kernel(const __grid_con
     if (lane == 0) {
       umma::prefetch_tensormap(&P.a);
       umma::prefetch_tensormap(&P.b);
-      uint32_t it = 0;  // K blocks loaded so far (ring position)
-      for (int u = blockIdx.x; u < nunits && !s_abort; u += gridDim.x) {
-        OzUnit w;
-        if (!oz_unit(P, u, w)) continue;
-        const int ns = w.high ? kOzS : 4;  // slices the unit's pairs use
-        for (int i = 0; i < w.nk; ++i, ++it) {
+      uint32_t it = 0;  // stages filled so far (ring position)
+      while (!s_abort) {
+        const int u = (int)atomicAdd(P.counter, 1u);
+        const bool end = u >= nunits;
+        OzUnit w{};
+        if (!end && !oz_unit(P, u, w)) continue;
+        // A T unit's stage holds one K block (8 slices of each operand), a U unit's two consecutive K blocks (4
+        // slices each, slot 4h + p for block h), so both kinds move 64 KB per stage.  A unit without K blocks still
+        // passes one empty stage, so that its tile's output is written.
+        const int ns = w.high ? kOzS : 4, per = w.high ? 1 : 2;
+        const int nstages = end ? 1 : max(1, (w.nk + per - 1) / per);
+        for (int i = 0; i < nstages; ++i, ++it) {
           const int s = it % kOStages;
           if (it >= kOStages && !umma::mbar_wait(&empty_bar[s], ((it / kOStages) - 1) & 1, P.limit_ns)) {
             set_status(P.st, kStatusBarrierTimeout, 0, 21);
@@ -237,34 +280,51 @@ __global__ void __launch_bounds__(kOThreads, 1) oz_pairs_kernel(const __grid_con
             break;
           }
           if (s_abort) break;
+          stage_unit[s] = end ? -1 : u;
           unsigned char* st = smem + (size_t)s * kOStageBytes;
-          const int k0 = (w.kb0 + i) * kOBK;
-          umma::mbar_arrive_expect_tx(&full_bar[s], (uint32_t)(2 * ns * kOSliceTile));
-          for (int p = 0; p < ns; ++p)
-            umma::tma_load_2d(st + p * kOSliceTile, &P.a, &full_bar[s], k0, p * P.M + w.m0);
-          for (int q = 0; q < ns; ++q)
-            umma::tma_load_2d(st + (kOzS + q) * kOSliceTile, &P.b, &full_bar[s], k0, q * P.N + w.n0);
+          const int nb = end ? 0 : max(0, min(per, w.nk - i * per));
+          umma::mbar_arrive_expect_tx(&full_bar[s], (uint32_t)(nb * 2 * ns * kOSliceTile));
+          for (int h = 0; h < nb; ++h) {
+            const int k0 = (w.kb0 + i * per + h) * kOBK;
+            for (int p = 0; p < ns; ++p)
+              umma::tma_load_2d(st + (h * ns + p) * kOSliceTile, &P.a, &full_bar[s], k0, p * P.M + w.m0);
+            for (int q = 0; q < ns; ++q)
+              umma::tma_load_2d(st + (kOzS + h * ns + q) * kOSliceTile, &P.b, &full_bar[s], k0, q * P.N + w.n0);
+          }
         }
+        if (end) break;
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       const uint32_t idesc = umma::idesc_i8(kOBM, kOBN);
       uint32_t it = 0, nu = 0;
-      for (int u = blockIdx.x; u < nunits && !s_abort; u += gridDim.x) {
-        OzUnit w;
-        if (!oz_unit(P, u, w)) continue;
+      while (!s_abort) {
+        int s = it % kOStages;
+        if (!umma::mbar_wait(&full_bar[s], (it / kOStages) & 1, P.limit_ns)) {
+          set_status(P.st, kStatusBarrierTimeout, 0, 23);
+          s_abort = 1;
+          break;
+        }
+        const int u = stage_unit[s];
         if (nu > 0 && !umma::mbar_wait(&free_bar, (nu - 1) & 1, P.limit_ns)) {
           set_status(P.st, kStatusBarrierTimeout, 0, 22);
           s_abort = 1;
           break;
         }
         umma::tc_fence_after();
+        meta_unit[nu & 1] = u;
+        umma::mbar_arrive(&meta_bar);
+        if (u < 0) break;
+        OzUnit w{};
+        oz_unit(P, u, w);
         const int dlo = w.high ? 6 : 2;
-        for (int i = 0; i < w.nk; ++i, ++it) {
-          const int s = it % kOStages;
-          if (!umma::mbar_wait(&full_bar[s], (it / kOStages) & 1, P.limit_ns)) {
-            set_status(P.st, kStatusBarrierTimeout, 0, 23);
+        const int ns = w.high ? kOzS : 4, per = w.high ? 1 : 2;
+        const int nstages = max(1, (w.nk + per - 1) / per);
+        for (int i = 0; i < nstages; ++i, ++it) {
+          s = it % kOStages;
+          if (i > 0 && !umma::mbar_wait(&full_bar[s], (it / kOStages) & 1, P.limit_ns)) {
+            set_status(P.st, kStatusBarrierTimeout, 0, 24);
             s_abort = 1;
             break;
           }
@@ -272,12 +332,16 @@ __global__ void __launch_bounds__(kOThreads, 1) oz_pairs_kernel(const __grid_con
           umma::tc_fence_after();
           const uint32_t sa = umma::smem_addr(smem + (size_t)s * kOStageBytes);
           const uint32_t sb = sa + kOzS * kOSliceTile;
-          for (int d = dlo; d < dlo + 4; ++d) {
-            const int p_lo = max(1, d - kOzS), p_hi = min(kOzS, d - 1);
-            for (int p = p_lo; p <= p_hi; ++p) {
-              const uint64_t ad = umma::desc_kmajor_sw32(sa + (p - 1) * kOSliceTile);
-              const uint64_t bd = umma::desc_kmajor_sw32(sb + (d - p - 1) * kOSliceTile);
-              umma::mma_i8(tmem + (uint32_t)(d - dlo) * kOBN, ad, bd, idesc, (i == 0 && p == p_lo) ? 0u : 1u);
+          const int nb = max(0, min(per, w.nk - i * per));
+          for (int h = 0; h < nb; ++h) {
+            for (int d = dlo; d < dlo + 4; ++d) {
+              const int p_lo = max(1, d - kOzS), p_hi = min(kOzS, d - 1);
+              for (int p = p_lo; p <= p_hi; ++p) {
+                const uint64_t ad = umma::desc_kmajor_sw32(sa + (h * ns + p - 1) * kOSliceTile);
+                const uint64_t bd = umma::desc_kmajor_sw32(sb + (h * ns + d - p - 1) * kOSliceTile);
+                const bool first = i == 0 && h == 0 && p == p_lo;
+                umma::mma_i8(tmem + (uint32_t)(d - dlo) * kOBN, ad, bd, idesc, first ? 0u : 1u);
+              }
             }
           }
           umma::mma_commit(&empty_bar[s]);
@@ -288,50 +352,46 @@ __global__ void __launch_bounds__(kOThreads, 1) oz_pairs_kernel(const __grid_con
       }
     }
   } else {
-    // Epilogue warps 2..9: TMEM lane quarter warp % 4 (the rows), column half (warp - 2) / 4.
+    // Epilogue warps 2..9: TMEM lane quarter warp % 4 (the rows), column half (warp - 2) / 4.  The accumulators are
+    // read into registers and TMEM is handed back before the stores, which then overlap the next unit's MMAs.
     const int quarter = warp & 3, half = (warp - 2) >> 2;
     uint32_t nu = 0;
-    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
-      OzUnit w;
-      if (!oz_unit(P, u, w)) continue;
-      const bool ok = __all_sync(0xffffffffu, umma::mbar_wait(&done_bar, nu & 1, P.limit_ns) ? 1 : 0) != 0;
+    while (true) {
+      bool ok = __all_sync(0xffffffffu, umma::mbar_wait(&meta_bar, nu & 1, P.limit_ns) ? 1 : 0) != 0;
+      const int u = ok ? meta_unit[nu & 1] : -1;
+      if (ok && u >= 0) ok = __all_sync(0xffffffffu, umma::mbar_wait(&done_bar, nu & 1, P.limit_ns) ? 1 : 0) != 0;
       if (!ok) {
-        if (lane == 0) set_status(P.st, kStatusBarrierTimeout, 0, 24);
+        if (lane == 0) set_status(P.st, kStatusBarrierTimeout, 0, 25);
         s_abort = 1;
         break;
       }
+      if (u < 0) break;
+      OzUnit w{};
+      oz_unit(P, u, w);
       umma::tc_fence_after();
-      const int row = w.m0 + quarter * 32 + lane;
-      double* out = w.high ? P.T : P.U;
-      for (int c = half * 64; c < half * 64 + 64; c += 32) {
-        double acc[32];
-        if (w.nk > 0) {
-          uint32_t r[32];
-          const uint32_t base = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c;
-          umma::tmem_ld32(base, r);
+      double v0[32], v1[32];
+      const uint32_t base = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * 64);
+      if (w.nk > 0) {
+        oz_read_unit(base, v0);
+        oz_read_unit(base + 32u, v1);
+      } else {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) acc[j] = (double)(int)r[j];
-#pragma unroll
-          for (int a = 1; a < 4; ++a) {  // Horner in 2^7, exact: every partial sum is an integer below 2^53
-            umma::tmem_ld32(base + (uint32_t)(a * kOBN), r);
-#pragma unroll
-            for (int j = 0; j < 32; ++j) acc[j] = fma(acc[j], 128.0, (double)(int)r[j]);
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) acc[j] = 0.0;
-        }
-        if (row < P.M) {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int col = w.n0 + c + j;
-            if (col < P.N) out[row + (size_t)col * P.M] = acc[j];
-          }
-        }
+        for (int j = 0; j < 32; ++j) v0[j] = v1[j] = 0.0;
       }
       umma::tc_fence_before();
       __syncwarp();
       if (lane == 0) umma::mbar_arrive(&free_bar);
+      const int row = w.m0 + quarter * 32 + lane;
+      double* out = (w.high ? P.T : P.U) + row;
+      const int c0 = w.n0 + half * 64;
+      if (row < P.M) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          if (c0 + j < P.N) out[(size_t)(c0 + j) * P.M] = v0[j];
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          if (c0 + 32 + j < P.N) out[(size_t)(c0 + 32 + j) * P.M] = v1[j];
+      }
       ++nu;
     }
   }
@@ -405,7 +465,7 @@ bool g_oz_smem[64];
 size_t ozaki_work_bytes(int M, int N, int K) {
   const size_t kp = (size_t)oz_kp(K);
   return up256((size_t)kOzS * M * kp) + up256((size_t)kOzS * N * kp) + 2 * up256((size_t)M * N * 8) +
-         up256((size_t)(M + N) * 8) + 256;
+         up256((size_t)(M + N + 1) * 8) + 256;
 }
 
 cudaError_t ozaki_dgemm(const GemmDesc<double>& p, void* work, size_t work_bytes, DeviceStatus* st, uint64_t limit_ns,
@@ -424,7 +484,8 @@ cudaError_t ozaki_dgemm(const GemmDesc<double>& p, void* work, size_t work_bytes
   double* U = reinterpret_cast<double*>(w);
   w += up256((size_t)p.M * p.N * 8);
   unsigned long long* maxbits = reinterpret_cast<unsigned long long*>(w);
-  cudaError_t err = cudaMemsetAsync(maxbits, 0, (size_t)(p.M + p.N) * 8, s);
+  unsigned* counter = reinterpret_cast<unsigned*>(maxbits + p.M + p.N);
+  cudaError_t err = cudaMemsetAsync(maxbits, 0, (size_t)(p.M + p.N + 1) * 8, s);
   if (err != cudaSuccess) return err;
   if (K > 0) {
     OzPrep P;
@@ -463,6 +524,7 @@ cudaError_t ozaki_dgemm(const GemmDesc<double>& p, void* work, size_t work_bytes
     Q.mode = p.mode;
     Q.tiles_m = (p.M + kOBM - 1) / kOBM;
     Q.tiles = Q.tiles_m * ((p.N + kOBN - 1) / kOBN);
+    Q.counter = counter;
     Q.st = st;
     Q.limit_ns = limit_ns;
     int dev = 0, sms = 0;
