@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture
 def restore(xe):
-    keys = ("autotune", "reduction", "band_width", "precision", "ormtr_nb", "sytrd_grid")
+    keys = ("autotune", "reduction", "band_width", "precision", "ormtr_nb", "sytrd_grid", "dgemm_engine")
     old = {k: xe.get_option(k) for k in keys}
     yield xe
     for k, v in old.items():
@@ -30,7 +30,7 @@ def test_autotune_plan_and_solve(restore, precision):
     plan = xe.autotune(n, precision)
     assert plan is not None and plan["ms"] > 0
     assert plan["reduction"] in (1, 2) and plan["band_width"] in (16, 32, 64)
-    assert plan["ormtr_nb"] in (64, 128, 256) and plan["mixed_gemm"] in (0, 3)
+    assert plan["ormtr_nb"] in (64, 128, 256) and plan["mixed_gemm"] in (0, 3) and plan["dgemm"] in (0, 1)
     xe.set_option("autotune", 1)
     xe.set_option("precision", precision)
     h, s, lam = inputs.generalized(n, seed=91)

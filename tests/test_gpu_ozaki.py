@@ -7,12 +7,15 @@
     close as the FP64 DMMA engine's bound 2 K eps |op(A)| |op(B)| on the same data;
   - integer data is multiplied exactly; k = 0 gives beta C; a row holding a NaN or an Inf gives NaN in its row;
     K above 65000 is refused (the int32 accumulators' exactness bound);
-  - at n = 1788 against torch's FP64 product.
+  - at n = 1788 against torch's FP64 product;
+  - generalized solves whose large GEMMs (congruence, back-transform, refinement) run on the engine meet the FP64
+    path's bars against the LAPACK oracle (eigenvalues within 1e-10 Eh, density within 1e-9), in FP64 and mixed
+    precision.
 """
 import numpy as np
 import pytest
 
-from oracle import ozaki
+from oracle import inputs, lapack, metrics, ozaki
 
 pytestmark = pytest.mark.gpu
 
@@ -128,3 +131,20 @@ def test_ozaki_n1788_matches_fp64(oz):
     ref = B @ A  # the row-major views hold the transposes: C^T = B^T A^T
     absprod = B.abs() @ A.abs()
     assert bool(((C - ref).abs() <= 4 * n * 2.0 ** -53 * absprod).all())
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_solves_on_the_ozaki_engine_meet_the_fp64_bars(oz, precision):
+    xe = oz
+    old = xe.get_option("precision")
+    xe.set_option("precision", precision)
+    try:
+        n = 700
+        h, s, lam = inputs.generalized(n, seed=171)
+        w_ref, c_ref = lapack.sygvd_chain(h, s)
+        w, c, _, info = xe.dsygvd(h, s)
+        assert info == 0, xe.last_error()
+        assert np.max(np.abs(w - lam)) < 1e-10
+        assert metrics.density_error(c, c_ref, metrics.aufbau(n, n // 2)) < 1e-9
+    finally:
+        xe.set_option("precision", old)

@@ -38,7 +38,7 @@ std::atomic<long> g_mixed_gemm{3};    // FP32 GEMMs of the mixed solve: 0 CUDA c
 std::atomic<long> g_reduction{1};     // 1: one-stage resident sytrd + ormtr; 2: two-stage sy2sb + sb2st
 std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (16, 32, 64)
 std::atomic<long> g_autotune{0};      // 1: solves use the autotuned plan nearest their size (xtb_gpu_autotune)
-std::atomic<long> g_dgemm_engine{0};  // FP64 GEMMs of xtb_dgemm_device: 0 DMMA, 1 int8 slices on tcgen05 (Ozaki)
+std::atomic<long> g_dgemm_engine{0};  // FP64 GEMMs (solves and xtb_dgemm_device): 0 DMMA, 1 int8 tcgen05 (Ozaki)
 
 // The tunable choices of one solve.  A solve resolves its plan once (options, or the autotuned table) and every stage
 // reads it from t_plan; the plan's signature is part of the graph-cache key, so a captured graph is never replayed
@@ -49,10 +49,11 @@ struct Plan {
   int sytrd_grid = 0;  // CTAs of the resident reduction (0: one per SM)
   int ormtr_nb = 128;  // reflectors per compact-WY block of ormtr
   int mixed_gemm = 3;  // FP32 GEMM engine of the mixed path
+  int dgemm = 0;       // FP64 GEMM engine of the large GEMMs: 0 DMMA, 1 int8 Ozaki
   double ms = 0.0;     // measured time of the tuned plan
   long long sig() const {
     return (long long)reduction | (long long)band << 4 | (long long)sytrd_grid << 12 | (long long)ormtr_nb << 24 |
-           (long long)mixed_gemm << 36;
+           (long long)mixed_gemm << 36 | (long long)dgemm << 40;
   }
 };
 
@@ -68,6 +69,7 @@ Plan options_plan() {
   p.sytrd_grid = (int)g_sytrd_grid.load();
   p.ormtr_nb = (int)g_ormtr_nb.load();
   p.mixed_gemm = (int)g_mixed_gemm.load();
+  p.dgemm = (int)g_dgemm_engine.load();
   return p;
 }
 
@@ -466,14 +468,22 @@ void stage_backtransform(Call& k, const char* pre, int n, int m, const Reduction
 }
 
 // The tcgen05 engine for the FP32 GEMMs of an n x n mixed solve (passes from the mixed_gemm option; 0 = CUDA cores).
+// The GEMM engines of an n x n solve under the current plan: the FP32 tensor-core engine (mixed path) and the FP64
+// engine of the large GEMMs, with their workspaces.
 TcGemm tc_engine(Call& k, int n) {
   TcGemm tc;
-  tc.passes = t_plan.mixed_gemm;
-  if (tc.passes == 0) return tc;
-  tc.work_elems = tc_work_elems(n);
-  tc.work = k.template dev<float>("tc.work", tc.work_elems);
   tc.st = k.c->d_status;
   tc.limit_ns = wait_limit_ns();
+  tc.passes = t_plan.mixed_gemm;
+  if (tc.passes != 0) {
+    tc.work_elems = tc_work_elems(n);
+    tc.work = k.template dev<float>("tc.work", tc.work_elems);
+  }
+  tc.dgemm = t_plan.dgemm;
+  if (tc.dgemm == 1 && ozaki_eligible(n, n, n)) {
+    tc.oz_bytes = ozaki_work_bytes(n, n, n);
+    tc.oz_work = k.template dev<char>("ozaki.work", tc.oz_bytes);
+  }
   return tc;
 }
 
@@ -515,21 +525,23 @@ void solve_factored_fp64(Call& k, int n, double* h, const double* x, int ldx, do
   double* hp = k.template dev<double>("gv.Hp", (size_t)n * n);
   double* z = k.template dev<double>("gv.Z", (size_t)n * n);
   double* e = k.template dev<double>("gv.e", (size_t)n);
+  TcGemm tc = tc_engine(k, n);
+  tc.passes = 0;  // FP64 problems only
   if (!k.ok()) return;
   // G = H X (X upper), then H' = X^T G on the upper tiles, symmetrised for the reduction.
   GemmDesc<double> p = gemm_problem<double>(n, n, n, 1.0, h, n, 0, x, ldx, 0, 0.0, t, n, kTriBUpper);
-  if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "congruence 1");
+  if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "congruence 1");
   p = gemm_problem<double>(n, n, n, 1.0, x, ldx, 1, t, n, 0, 0.0, hp, n, kTriALower | kCUpper);
-  if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "congruence 2");
+  if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "congruence 2");
   if (k.ok()) symmetrize_upper<double>(n, hp, n, h, n, k.s);
   k.mark("congruence");
-  const Reduction<double> red = stage_reduce<double>(k, "gv.", n, h, w, e, TcGemm());
+  const Reduction<double> red = stage_reduce<double>(k, "gv.", n, h, w, e, tc);
   stage_stedc(k, n, w, e, z, n);
   k.mark("stedc");
-  stage_backtransform<double>(k, "gv.", n, n, red, z, n, TcGemm());
+  stage_backtransform<double>(k, "gv.", n, n, red, z, n, tc);
   // C = X Z (X upper).
   p = gemm_problem<double>(n, n, n, 1.0, x, ldx, 0, z, n, 0, 0.0, c, n, kTriAUpper);
-  if (k.ok()) k.check(gemm_group<double>(k.c->arena, &p, 1, k.s), "back-transform");
+  if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "back-transform");
   k.mark("trmm");
 }
 
@@ -1300,7 +1312,7 @@ int xtb_gpu_autotune(int n, int precision, void* stream) {
   }
   // Candidates, one coordinate at a time: the reduction (one stage with the resident kernel on all / 3/4 / 1/2 of the
   // SMs; two stages with band width 16 / 32 / 64), then ormtr's block size for the one-stage winner, then the FP32
-  // GEMM engine of the mixed path.
+  // GEMM engine of the mixed path, then the FP64 engine of the large GEMMs (DMMA or int8 Ozaki).
   const long prec0 = g_precision.load();
   g_precision = precision;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1370,6 +1382,12 @@ int xtb_gpu_autotune(int n, int precision, void* stream) {
     p.mixed_gemm = r.mixed_gemm == 3 ? 0 : 3;
     consider(p);
   }
+  if (ozaki_eligible(n, n, n)) {  // the FP64 engine of the large GEMMs (congruence, back-transform, refinement)
+    const Plan r = best;
+    Plan p = r;
+    p.dgemm = r.dgemm == 1 ? 0 : 1;
+    consider(p);
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   g_precision = prec0;
@@ -1391,8 +1409,8 @@ int xtb_gpu_tuned_plan(int n, int precision, char* buf, int len) {
   if (it == g_plans.end()) return -1;
   const Plan& p = it->second;
   const int w = std::snprintf(buf, buf && len > 0 ? (size_t)len : 0,
-                              "reduction=%d band_width=%d sytrd_grid=%d ormtr_nb=%d mixed_gemm=%d ms=%.4f",
-                              p.reduction, p.band, p.sytrd_grid, p.ormtr_nb, p.mixed_gemm, p.ms);
+                              "reduction=%d band_width=%d sytrd_grid=%d ormtr_nb=%d mixed_gemm=%d dgemm=%d ms=%.4f",
+                              p.reduction, p.band, p.sytrd_grid, p.ormtr_nb, p.mixed_gemm, p.dgemm, p.ms);
   return w;
 }
 

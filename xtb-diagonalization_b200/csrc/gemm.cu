@@ -2,6 +2,8 @@
 // by tile::gemm_tile (FP64 DMMA, four-stage cp.async pipeline; gemm_tile.cuh).
 #include "gemm.cuh"
 
+#include <vector>
+
 #include "gemm_tile.cuh"
 #include "kernels.h"
 
@@ -127,8 +129,25 @@ cudaError_t gemm_group(DescArena& arena, const GemmDesc<T>* probs, int nprob, cu
   return cudaGetLastError();
 }
 
-cudaError_t gemm_run(DescArena& arena, const TcGemm&, const GemmDesc<double>* probs, int nprob, cudaStream_t s) {
-  return gemm_group<double>(arena, probs, nprob, s);
+cudaError_t gemm_run(DescArena& arena, const TcGemm& tc, const GemmDesc<double>* probs, int nprob, cudaStream_t s) {
+  if (tc.dgemm != 1 || !tc.oz_work) return gemm_group<double>(arena, probs, nprob, s);
+  // The eligible problems run one after another on the Ozaki engine (sharing its workspace), the rest as one group.
+  auto takes = [&](const GemmDesc<double>& p) {
+    return ozaki_eligible(p.M, p.N, p.K) && ozaki_work_bytes(p.M, p.N, p.K) <= tc.oz_bytes;
+  };
+  int neligible = 0;
+  for (int i = 0; i < nprob; ++i) neligible += takes(probs[i]) ? 1 : 0;
+  if (neligible == 0) return gemm_group<double>(arena, probs, nprob, s);
+  std::vector<GemmDesc<double>> rest;
+  for (int i = 0; i < nprob; ++i) {
+    if (!takes(probs[i])) {
+      rest.push_back(probs[i]);
+      continue;
+    }
+    const cudaError_t err = ozaki_dgemm(probs[i], tc.oz_work, tc.oz_bytes, tc.st, tc.limit_ns, s);
+    if (err != cudaSuccess) return err;
+  }
+  return rest.empty() ? cudaSuccess : gemm_group<double>(arena, rest.data(), (int)rest.size(), s);
 }
 
 cudaError_t gemm_run(DescArena& arena, const TcGemm& tc, const GemmDesc<float>* probs, int nprob, cudaStream_t s) {

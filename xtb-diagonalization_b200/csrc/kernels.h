@@ -93,15 +93,22 @@ cudaError_t ozaki_dgemm(const GemmDesc<double>& p, void* work, size_t work_bytes
                         cudaStream_t s);
 
 struct DescArena;
-// Which engine runs a stage's GEMMs: passes 0 = the grouped GEMM (FP64 DMMA / FP32 CUDA cores); for FP32 problems
-// passes 1 or 3 = the tcgen05 engine.
+// Which engine runs a stage's GEMMs.  FP32 problems: passes 0 = the grouped GEMM on the CUDA cores, 1 or 3 = the
+// tcgen05 TF32 engine.  FP64 problems: dgemm 0 = the grouped DMMA GEMM, 1 = the int8 Ozaki engine for the problems
+// large enough to pay for its slicing (ozaki_eligible), DMMA for the rest.
 struct TcGemm {
   int passes = 0;
   float* work = nullptr;
   size_t work_elems = 0;
+  int dgemm = 0;
+  void* oz_work = nullptr;
+  size_t oz_bytes = 0;
   DeviceStatus* st = nullptr;
   uint64_t limit_ns = 0;
 };
+// The Ozaki engine slices both operands of every call (about 32 bytes of traffic per element), which a GEMM with a
+// small dimension does not amortise: it takes problems with M, N and K all >= 512 (and K within its bound).
+inline bool ozaki_eligible(int M, int N, int K) { return M >= 512 && N >= 512 && K >= 512 && K <= 65000; }
 cudaError_t gemm_run(DescArena& arena, const TcGemm& tc, const GemmDesc<double>* probs, int nprob, cudaStream_t s);
 cudaError_t gemm_run(DescArena& arena, const TcGemm& tc, const GemmDesc<float>* probs, int nprob, cudaStream_t s);
 
@@ -203,7 +210,8 @@ cudaError_t dk_adjoint(int n, const double* c, const double* e, double mu, doubl
 size_t refine_work_elems(int n);
 // u (may be NULL): the upper Cholesky factor of s (ld ldu); with it C^T S C is formed as (U C)^T (U C).
 // tc (may be NULL): with a tensor-core engine, every step's update C (I + E) but the last runs as C D (the clusters'
-// blocks, FP64) + C F (the first-order remainder, on the tensor cores); the last update stays FP64.
+// blocks, FP64) + C F (the first-order remainder, on the tensor cores); the last update stays FP64.  tc->dgemm
+// selects the engine of the FP64 GEMMs (DMMA without tc).
 cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s, int lds, const double* u, int ldu,
                                double* c, int ldc, double* w, int iters, double* work, DescArena& arena,
                                cudaStream_t st, const TcGemm* tc = nullptr);

@@ -367,6 +367,9 @@ cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s,
   float* c32 = f32 + nn;
   float* p32 = c32 + nn;
   const bool tc_update = tc && tc->passes > 0;
+  TcGemm tc64;  // the FP64 GEMMs: the engine the caller chose (DMMA without one)
+  if (tc) tc64 = *tc;
+  tc64.passes = 0;
   // The current iterate alternates between cur and nxt; the result is scattered into c in ascending order.
   const double* cur = c;
   int ldcur = ldc;
@@ -380,11 +383,11 @@ cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s,
     p[0] = gemm_problem<double>(n, n, n, 1.0, h, ldh, 0, cur, ldcur, 0, 0.0, t1, n);
     p[1] = u ? gemm_problem<double>(n, n, n, 1.0, u, ldu, 0, cur, ldcur, 0, 0.0, t2, n, kTriAUpper)
              : gemm_problem<double>(n, n, n, 1.0, s, lds, 0, cur, ldcur, 0, 0.0, t2, n);
-    if ((err = gemm_group<double>(arena, p, 2, st)) != cudaSuccess) return err;
+    if ((err = gemm_run(arena, tc64, p, 2, st)) != cudaSuccess) return err;
     p[0] = gemm_problem<double>(n, n, n, 1.0, cur, ldcur, 1, t1, n, 0, 0.0, A, n, kCUpper);
     p[1] = u ? gemm_problem<double>(n, n, n, 1.0, t2, n, 1, t2, n, 0, 0.0, B, n, kCUpper)
              : gemm_problem<double>(n, n, n, 1.0, cur, ldcur, 1, t2, n, 0, 0.0, B, n, kCUpper);
-    if ((err = gemm_group<double>(arena, p, 2, st)) != cudaSuccess) return err;
+    if ((err = gemm_run(arena, tc64, p, 2, st)) != cudaSuccess) return err;
     mirror_upper_inplace<double>(n, A, n, st);
     mirror_upper_inplace<double>(n, B, n, st);
     if ((err = cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), st)) != cudaSuccess) return err;
@@ -396,7 +399,7 @@ cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s,
     // the tensor cores' FP32 accumulation); the last step's update stays FP64, which sets the final accuracy.
     if (!tc_update || it == iters - 1) {
       p[0] = gemm_problem<double>(n, n, n, 1.0, cur, ldcur, 0, M, n, 0, 0.0, nxt, n);
-      if ((err = gemm_group<double>(arena, p, 1, st)) != cudaSuccess) return err;
+      if ((err = gemm_run(arena, tc64, p, 1, st)) != cudaSuccess) return err;
     } else {
       // nxt = C M = C D + C F: the clusters' rotations in FP64, the small first-order remainder F on the tensor
       // cores.
