@@ -555,7 +555,7 @@ def run_batch_section(args, dev, stream):
     elems = sum(n * n for n in sizes)
     return {
         "count": count, "sizes": "uniform integers in [124, 1788], seed 3; problem i built with seed 1000 + i",
-        "workers": workers, "solves_per_s": round(count / (ms_batch * 1e-3), 2), "ms_per_batch": round(ms_batch, 2),
+        "workers": workers, "batch_grid": xtbeig.get_option("batch_grid"), "solves_per_s": round(count / (ms_batch * 1e-3), 2), "ms_per_batch": round(ms_batch, 2),
         "steps": steps, "warmup": 3, "gpu_launches_per_batch": int(launches // steps),
         "one_at_a_time_solves_per_s": round(count / (one_ms * 1e-3), 2), "one_at_a_time_ms": round(one_ms, 2),
         "speedup_vs_one_at_a_time": round(one_ms / ms_batch, 3), "per_size_ms_alone": bins,

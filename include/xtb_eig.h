@@ -177,7 +177,7 @@ int xtb_dsygvd_density_adjoint_batched(int count, const int* n, const double* co
  * compact-WY block, default 128), "wait_limit_ms" (device wait time limit, default 2000), "stage_timing" (1: record
  * CUDA events at stage boundaries; read with xtb_gpu_stage_*), "graphs" (default 1: a device-pointer solve repeated
  * on the same buffers and non-NULL stream is captured into a CUDA graph on its second call and replayed after),
- * "batch_workers" (host threads, each with its own stream, that the batch calls spread problems over; default 4),
+ * "batch_workers" (host threads, each with its own stream, that the batch calls spread problems over; default 8),
  * "precision" (64, default: FP64 throughout; 32: the generalized solves run the reduction chain in FP32 - congruence,
  * resident sytrd, ormtr, back-transform; Cholesky and the tridiagonal eigensolve stay FP64 - then refine C and e in
  * FP64 as xtb_dsygvd_refine_device does), "refine_iters" (refinement steps of the mixed path, default 2),
@@ -185,7 +185,10 @@ int xtb_dsygvd_density_adjoint_batched(int count, const int* n, const double* co
  * 0 = FP32 on the CUDA cores), "reduction" (1 = one-stage resident sytrd, default; 2 = two-stage sy2sb + sb2st),
  * "band_width" (two-stage band width 16, 32 default, 64), "autotune" (1: use xtb_gpu_autotune's plans),
  * "dgemm_engine" (the FP64 GEMMs of xtb_dgemm_device and the solves' large GEMMs - congruence, back-transform,
- * refinement, all of M, N, K >= 512: 0 = DMMA, default; 1 = int8 Ozaki slices on the tcgen05 tensor cores).
+ * refinement, all of M, N, K >= 512: 0 = DMMA, default; 1 = int8 Ozaki slices on the tcgen05 tensor cores),
+ * "batch_grid" (1, default: inside the batch calls, each problem's resident reduction takes the fewest CTAs that
+ * hold its rows in shared memory, so that problems run side by side; the results are bit for bit those of single
+ * solves; 0 = the single-solve grid).
  * Returns 0, -1 for an unknown name, or -2 for a value out of range. */
 int xtb_gpu_set_option(const char* name, long value);
 long xtb_gpu_get_option(const char* name);

@@ -152,6 +152,34 @@ def test_batched_uneven(xe, workers):
         np.testing.assert_array_equal(np.triu(ui), np.triu(u1))
 
 
+def test_batched_grid_policy(xe):
+    """Option "batch_grid" = 1: inside a batch each resident reduction takes the fewest CTAs that hold its rows in
+    shared memory (a handful for small problems instead of one per four rows).  Every problem meets the FP64 bars,
+    and the result is bit for bit the single-problem call's: the reduction's sums do not depend on its grid."""
+    sizes = [37, 130, 64, 200, 311, 96, 640]
+    probs = _batch_problems(sizes, seed0=5000)
+    old = {k: xe.get_option(k) for k in ("batch_grid", "batch_workers", "precision")}
+    try:
+        xe.set_option("batch_workers", 4)
+        for precision in (64, 32):
+            xe.set_option("precision", precision)
+            xe.set_option("batch_grid", 1)
+            w, c, u, info, ret = xe.dsygvd_batched([p[0] for p in probs], [p[1] for p in probs])
+            assert ret == 0 and np.all(info == 0)
+            xe.set_option("batch_grid", 0)
+            for (h, s, lam), wi, ci in zip(probs, w, c):
+                n = h.shape[0]
+                assert np.max(np.abs(wi - lam)) < 1e-10
+                assert metrics.backward_error(h, s, wi, ci) < 10
+                w1, c1, _, info1 = xe.dsygvd(h, s)
+                assert info1 == 0
+                np.testing.assert_array_equal(wi, w1)
+                np.testing.assert_array_equal(ci, c1)
+    finally:
+        for k, v in old.items():
+            xe.set_option(k, v)
+
+
 def test_batched_failure_is_per_problem(xe):
     """A non-SPD overlap in one problem fails that problem only (info = n + failing column, as dsygvd) and the call
     returns its info; the other problems are solved."""

@@ -31,13 +31,14 @@ std::atomic<long> g_ormtr_nb{128};
 std::atomic<long> g_wait_ms{2000};
 std::atomic<long> g_stage_timing{0};
 std::atomic<long> g_graphs{1};
-std::atomic<long> g_batch_workers{4};
+std::atomic<long> g_batch_workers{8};
 std::atomic<long> g_precision{64};    // 64: FP64 throughout; 32: FP32 reduction chain + FP64 refinement
 std::atomic<long> g_refine_iters{2};
 std::atomic<long> g_mixed_gemm{3};    // FP32 GEMMs of the mixed solve: 0 CUDA cores, 1 TF32, 3 3xTF32 (tcgen05)
 std::atomic<long> g_reduction{1};     // 1: one-stage resident sytrd + ormtr; 2: two-stage sy2sb + sb2st
 std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (16, 32, 64)
 std::atomic<long> g_autotune{0};      // 1: solves use the autotuned plan nearest their size (xtb_gpu_autotune)
+std::atomic<long> g_batch_grid{1};    // 1: batch workers size each resident reduction's grid to its matrix
 std::atomic<long> g_dgemm_engine{0};  // FP64 GEMMs (solves and xtb_dgemm_device): 0 DMMA, 1 int8 tcgen05 (Ozaki)
 
 // The tunable choices of one solve.  A solve resolves its plan once (options, or the autotuned table) and every stage
@@ -50,10 +51,11 @@ struct Plan {
   int ormtr_nb = 128;  // reflectors per compact-WY block of ormtr
   int mixed_gemm = 3;  // FP32 GEMM engine of the mixed path
   int dgemm = 0;       // FP64 GEMM engine of the large GEMMs: 0 DMMA, 1 int8 Ozaki
+  int batch_grid = 0;  // 1: a batch worker's solve, its resident reduction sized to its matrix (sytrd_grid 0)
   double ms = 0.0;     // measured time of the tuned plan
   long long sig() const {
     return (long long)reduction | (long long)band << 4 | (long long)sytrd_grid << 12 | (long long)ormtr_nb << 24 |
-           (long long)mixed_gemm << 36 | (long long)dgemm << 40;
+           (long long)mixed_gemm << 36 | (long long)dgemm << 40 | (long long)batch_grid << 41;
   }
 };
 
@@ -61,6 +63,7 @@ std::mutex g_plan_mu;
 std::map<std::pair<int, int>, Plan> g_plans;  // (precision, n) -> tuned plan
 thread_local Plan t_plan;
 thread_local const Plan* t_force_plan = nullptr;  // the autotuner's candidate under test
+thread_local int t_batch_workers = 0;              // > 1 while this thread is one of a batch call's workers
 
 Plan options_plan() {
   Plan p;
@@ -75,7 +78,7 @@ Plan options_plan() {
 
 // The plan of a solve of size n: the autotuner's candidate while it measures, else the tuned plan of the nearest
 // tuned size (log scale) when the autotune option is on, else the options.
-Plan plan_for(int n, int precision) {
+Plan plan_for_solo(int n, int precision) {
   if (t_force_plan) return *t_force_plan;
   if (g_autotune.load()) {
     std::lock_guard<std::mutex> lock(g_plan_mu);
@@ -92,6 +95,11 @@ Plan plan_for(int n, int precision) {
     if (best) return *best;
   }
   return options_plan();
+}
+Plan plan_for(int n, int precision) {
+  Plan p = plan_for_solo(n, precision);
+  p.batch_grid = (t_batch_workers > 1 && g_batch_grid.load() == 1 && p.sytrd_grid == 0 && !t_force_plan) ? 1 : 0;
+  return p;
 }
 std::atomic<long long> g_launches{0};
 thread_local long long t_launches = 0;  // this thread's launches: a graph capture counts its own, not other threads'
@@ -308,7 +316,15 @@ template <typename T>
 void stage_sytrd(Call& k, int n, const T* dfull, int ldf, T* dout, int lda, T* d, T* e, T* tau) {
   if (!k.ok() || n <= 0) return;
   const size_t smem_cap = k.c->max_smem > 2048 ? k.c->max_smem - 2048 : k.c->max_smem;
-  SytrdPlan pl = sytrd_plan<T>(n, k.c->num_sms, smem_cap, t_plan.sytrd_grid);
+  int grid = t_plan.sytrd_grid;
+  if (grid == 0 && t_plan.batch_grid == 1) {
+    // Inside a batch the reductions of several problems share the GPU: each takes the fewest CTAs that still hold
+    // its rows in shared memory (with a margin), which also makes its grid barrier cheaper, and leaves the other SMs
+    // to the problems beside it.
+    const size_t bytes = (size_t)n * n * sizeof(T), per_cta = smem_cap * 4 / 5;
+    grid = (int)std::min<size_t>((size_t)k.c->num_sms, std::max<size_t>(4, (bytes + per_cta - 1) / per_cta));
+  }
+  SytrdPlan pl = sytrd_plan<T>(n, k.c->num_sms, smem_cap, grid);
   if (!pl.supported) {
     k.check(cudaErrorInvalidValue, "sytrd: size not supported");
     return;
@@ -336,7 +352,8 @@ void stage_sytrd(Call& k, int n, const T* dfull, int ldf, T* dout, int lda, T* d
     p.grows = k.template dev<T>("sytrd.rows", (size_t)pl.grid * pl.rows_per_cta * pl.ldr);
     if (!k.ok()) return;
   }
-  k.check(cudaMemsetAsync(ctr, 0, 64 * sizeof(unsigned), k.s), "sytrd counter");  if (k.ok()) k.check(sytrd_launch<T>(p, pl, k.s), "sytrd launch");
+  k.check(cudaMemsetAsync(ctr, 0, 64 * sizeof(unsigned), k.s), "sytrd counter");
+  if (k.ok()) k.check(sytrd_launch<T>(p, pl, k.s), "sytrd launch");
 }
 
 // ormtr's compact-WY block size: the plan's, clamped so that a block's factor ((nb^2 + nb) elements) fits in shared
@@ -997,6 +1014,7 @@ int run_batch(int count, const int* n, int* info, const std::function<int(int)>&
   std::vector<std::string> msg(count);
   pool().run(nw, [&](int wk) {
     const cudaError_t e = cudaSetDevice(dev);
+    t_batch_workers = nw;
     for (int i : lists[wk]) {
       if (e != cudaSuccess) {
         inf[i] = -1000 - (int)e;
@@ -1572,6 +1590,11 @@ int xtb_gpu_set_option(const char* name, long value) {
     g_dgemm_engine = value;
     return 0;
   }
+  if (!std::strcmp(name, "batch_grid")) {
+    if (value != 0 && value != 1) return -2;
+    g_batch_grid = value;
+    return 0;
+  }
   return -1;
 }
 
@@ -1590,6 +1613,7 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "band_width")) return g_band_width;
   if (!std::strcmp(name, "autotune")) return g_autotune;
   if (!std::strcmp(name, "dgemm_engine")) return g_dgemm_engine;
+  if (!std::strcmp(name, "batch_grid")) return g_batch_grid;
   return -1;
 }
 
