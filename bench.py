@@ -273,6 +273,7 @@ def run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush):
         solve()
         stages = xtbeig.stage_times()
         xtbeig.set_option("stage_timing", 0)
+        solve()  # untimed: the stage-timed solve ran eagerly, so this one may (re)capture the solve's graph
         K = max(1, args.steps // 2)
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
         torch.cuda.nvtx.range_push("mixed_timed")
@@ -322,6 +323,7 @@ def run_variant_section(args, dev, stream, H0, S0, lam_t, flush, options, steps=
         solve()
         stages = xtbeig.stage_times()
         xtbeig.set_option("stage_timing", 0)
+        solve()  # untimed: the stage-timed solve ran eagerly, so this one may (re)capture the solve's graph
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         for i in range(steps):
             flush.zero_()
@@ -641,6 +643,8 @@ def run_ours(args):
     solve()
     stages = xtbeig.stage_times()
     xtbeig.set_option("stage_timing", 0)
+    solve()  # untimed: the stage-timed solve ran eagerly, so this one may (re)capture the solve's graph
+    torch.cuda.synchronize(dev)
 
     # Timed region.
     gpu_uuid = str(torch.cuda.get_device_properties(dev).uuid)

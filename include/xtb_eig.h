@@ -117,13 +117,13 @@ int xtb_dsygvd_refine_device(int n, const double* h, int ldh, const double* s, i
 int xtb_sgemm_tc_device(int transa, int transb, int m, int n, int k, float alpha, const float* a, int lda,
                         const float* b, int ldb, float beta, float* c, int ldc, int passes, void* stream);
 
-/* FP64 GEMM, DEVICE pointers, column-major as BLAS dgemm: C = alpha op(A) op(B) + beta C.  With the option
- * "dgemm_engine" 0 (default) on the FP64 tensor cores (DMMA), the engine of every FP64 GEMM-shaped stage (congruence,
- * ormtr, back-transform, refinement, D&C merges; the reference calls Accelerate dgemm for them, e.g.
- * Sources/Diagonalization/Stages/WYTransform.swift:22-79); with 1 on the int8 tcgen05 tensor cores by the Ozaki
- * splitting (rows of op(A) and columns of op(B) in 8 power-of-two scaled 7-bit slices, 36 exact int8 slice products;
- * k <= 65000), accurate to a small multiple of 2^-56 k max|op(A)(i,:)| max|op(B)(:,j)|.  Queued on `stream` and
- * synchronised.  Returns 0, -(argument position), -1000 - cudaError, or a device status code. */
+/* FP64 GEMM, DEVICE pointers, column-major as BLAS dgemm: C = alpha op(A) op(B) + beta C (the reference calls
+ * Accelerate dgemm for its GEMM-shaped stages, e.g. Sources/Diagonalization/Stages/WYTransform.swift:22-79).  Two
+ * engines, chosen by the option "dgemm_engine": the FP64 tensor cores (DMMA), and the int8 tcgen05 tensor cores by
+ * the Ozaki splitting (rows of op(A) and columns of op(B) in 8 power-of-two scaled 7-bit slices, 36 exact int8 slice
+ * products; k <= 65000), accurate to a small multiple of 2^-56 k max|op(A)(i,:)| max|op(B)(:,j)| and reproducible bit
+ * for bit.  0 = DMMA; 1 (default) = Ozaki when m, n and k are all >= 512, DMMA below; 2 = Ozaki always.  Queued on
+ * `stream` and synchronised.  Returns 0, -(argument position), -1000 - cudaError, or a device status code. */
 int xtb_dgemm_device(int transa, int transb, int m, int n, int k, double alpha, const double* a, int lda,
                      const double* b, int ldb, double beta, double* c, int ldc, void* stream);
 
@@ -185,7 +185,8 @@ int xtb_dsygvd_density_adjoint_batched(int count, const int* n, const double* co
  * 0 = FP32 on the CUDA cores), "reduction" (1 = one-stage resident sytrd, default; 2 = two-stage sy2sb + sb2st),
  * "band_width" (two-stage band width 16, 32 default, 64), "autotune" (1: use xtb_gpu_autotune's plans),
  * "dgemm_engine" (the FP64 GEMMs of xtb_dgemm_device and the solves' large GEMMs - congruence, back-transform,
- * refinement, all of M, N, K >= 512: 0 = DMMA, default; 1 = int8 Ozaki slices on the tcgen05 tensor cores),
+ * refinement: 0 = DMMA; 1 = int8 Ozaki slices on the tcgen05 tensor cores for GEMMs with all of M, N, K >= 512,
+ * default; 2 = the same, and xtb_dgemm_device uses Ozaki at every size),
  * "batch_grid" (1, default: inside the batch calls, each problem's resident reduction takes the fewest CTAs that
  * hold its rows in shared memory, so that problems run side by side; the results are bit for bit those of single
  * solves; 0 = the single-solve grid).

@@ -1,4 +1,5 @@
-"""GPU checks of the FP64 GEMM from int8 tcgen05 products (option "dgemm_engine" = 1 of xtb_dgemm_device).
+"""GPU checks of the FP64 GEMM from int8 tcgen05 products (option "dgemm_engine" = 2 of xtb_dgemm_device: Ozaki at
+every size; the default 1 takes it from 512^3 up).
 
   - bit for bit against the numpy emulation of the same splitting (oracle/ozaki.py) for every transpose combination,
     ragged sizes (M, N not multiples of the 128 x 64 tile, K not a multiple of the 64-deep K block), padded leading
@@ -23,7 +24,7 @@ pytestmark = pytest.mark.gpu
 @pytest.fixture
 def oz(xe):
     old = xe.get_option("dgemm_engine")
-    xe.set_option("dgemm_engine", 1)
+    xe.set_option("dgemm_engine", 2)
     yield xe
     xe.set_option("dgemm_engine", old)
 

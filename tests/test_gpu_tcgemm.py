@@ -116,11 +116,18 @@ def _run_d(xe, ta, tb, m, n, k, alpha, beta, seed):
     return C.T, ref, absprod
 
 
+@pytest.mark.parametrize("engine", [0, 1])
 @pytest.mark.parametrize("ta,tb", [(0, 0), (1, 0), (0, 1), (1, 1)])
 @pytest.mark.parametrize("mnk", [(1, 1, 1), (63, 65, 17), (130, 257, 129), (600, 500, 700)])
-def test_dgemm_matches_fp64(xe, ta, tb, mnk):
-    """xtb_dgemm_device (FP64 DMMA) against torch's FP64 product: elementwise within 2 k eps |op(A)| |op(B)|."""
+def test_dgemm_matches_fp64(xe, ta, tb, mnk, engine):
+    """xtb_dgemm_device against torch's FP64 product, elementwise within 2 k eps |op(A)| |op(B)|: engine 0 (FP64
+    DMMA) at every size, engine 1 (the default: int8 Ozaki from 512^3 up, DMMA below)."""
     m, n, k = mnk
-    out, ref, absprod = _run_d(xe, ta, tb, m, n, k, 1.25, -0.5, seed=m + 3 * n + 7 * k + ta + 2 * tb)
+    old = xe.get_option("dgemm_engine")
+    xe.set_option("dgemm_engine", engine)
+    try:
+        out, ref, absprod = _run_d(xe, ta, tb, m, n, k, 1.25, -0.5, seed=m + 3 * n + 7 * k + ta + 2 * tb)
+    finally:
+        xe.set_option("dgemm_engine", old)
     bound = 2 * (k + 2) * 2.0 ** -53 * absprod + 1e-300
     assert bool(((out - ref).abs() <= bound).all())

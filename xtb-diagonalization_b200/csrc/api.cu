@@ -39,7 +39,7 @@ std::atomic<long> g_reduction{1};     // 1: one-stage resident sytrd + ormtr; 2:
 std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (16, 32, 64)
 std::atomic<long> g_autotune{0};      // 1: solves use the autotuned plan nearest their size (xtb_gpu_autotune)
 std::atomic<long> g_batch_grid{1};    // 1: batch workers size each resident reduction's grid to its matrix
-std::atomic<long> g_dgemm_engine{0};  // FP64 GEMMs (solves and xtb_dgemm_device): 0 DMMA, 1 int8 tcgen05 (Ozaki)
+std::atomic<long> g_dgemm_engine{1};  // FP64 GEMMs: 0 DMMA, 1 Ozaki (int8 tcgen05) where eligible, 2 Ozaki always
 
 // The tunable choices of one solve.  A solve resolves its plan once (options, or the autotuned table) and every stage
 // reads it from t_plan; the plan's signature is part of the graph-cache key, so a captured graph is never replayed
@@ -50,12 +50,12 @@ struct Plan {
   int sytrd_grid = 0;  // CTAs of the resident reduction (0: one per SM)
   int ormtr_nb = 128;  // reflectors per compact-WY block of ormtr
   int mixed_gemm = 3;  // FP32 GEMM engine of the mixed path
-  int dgemm = 0;       // FP64 GEMM engine of the large GEMMs: 0 DMMA, 1 int8 Ozaki
+  int dgemm = 0;       // FP64 GEMM engine of the large GEMMs: 0 DMMA, 1 or 2 int8 Ozaki
   int batch_grid = 0;  // 1: a batch worker's solve, its resident reduction sized to its matrix (sytrd_grid 0)
   double ms = 0.0;     // measured time of the tuned plan
   long long sig() const {
     return (long long)reduction | (long long)band << 4 | (long long)sytrd_grid << 12 | (long long)ormtr_nb << 24 |
-           (long long)mixed_gemm << 36 | (long long)dgemm << 40 | (long long)batch_grid << 41;
+           (long long)mixed_gemm << 36 | (long long)dgemm << 40 | (long long)batch_grid << 42;
   }
 };
 
@@ -496,7 +496,7 @@ TcGemm tc_engine(Call& k, int n) {
     tc.work_elems = tc_work_elems(n);
     tc.work = k.template dev<float>("tc.work", tc.work_elems);
   }
-  tc.dgemm = t_plan.dgemm;
+  tc.dgemm = t_plan.dgemm != 0 ? 1 : 0;
   if (tc.dgemm == 1 && ozaki_eligible(n, n, n)) {
     tc.oz_bytes = ozaki_work_bytes(n, n, n);
     tc.oz_work = k.template dev<char>("ozaki.work", tc.oz_bytes);
@@ -1297,7 +1297,8 @@ int xtb_dgemm_device(int transa, int transb, int m, int n, int k_, double alpha,
   if (!c0) return t_state.last_code;
   Call k(c0, (cudaStream_t)stream, true);
   GemmDesc<double> p = gemm_problem<double>(m, n, k_, alpha, a, lda, transa, b, ldb, transb, beta, c, ldc);
-  if (g_dgemm_engine.load() == 1) {
+  const long engine = g_dgemm_engine.load();
+  if (engine == 2 || (engine == 1 && ozaki_eligible(m, n, k_))) {
     const size_t wb = ozaki_work_bytes(m, n, k_);
     char* w = k.dev<char>("ozaki.work", wb);
     if (k.ok()) k.check(ozaki_dgemm(p, w, wb, c0->d_status, wait_limit_ns(), k.s), "ozaki dgemm");
@@ -1586,7 +1587,7 @@ int xtb_gpu_set_option(const char* name, long value) {
     return 0;
   }
   if (!std::strcmp(name, "dgemm_engine")) {
-    if (value != 0 && value != 1) return -2;
+    if (value < 0 || value > 2) return -2;
     g_dgemm_engine = value;
     return 0;
   }
