@@ -39,97 +39,168 @@ struct PotrfParams {
   uint64_t limit_ns;
 };
 
-constexpr size_t kLeafElems = (size_t)2 * NB * (NB + 1) + NB;
+constexpr size_t kLeafElems = (size_t)2 * NB * (NB + 1) + NB + 8;  // U, X, 1 / U(k, k), a flag
 constexpr size_t kSmemBytes = (tile::smem_elems<double>() + kLeafElems) * sizeof(double);
 
 // Factor and invert the nb x nb (nb <= 64) diagonal block at (j0, j0) with the CTA's 128 threads: U in place in a,
-// X = U^-1 (upper, zero below the diagonal) into x.  Returns false (all threads) on a non-positive pivot.
+// X = U^-1 (upper; x's strict lower part is left as it is) into x.  Returns false (all threads) on a pivot that is
+// not > 0, after recording kStatusNotSPD with the global column (1-based).  The block is the kernel's critical path,
+// so it is factored by 8-column panels (three barriers per panel instead of two per column): the panel's 8 x 8
+// diagonal block by one warp with shuffles, its block row by a triangular solve per column, then the rank-8 update
+// of the trailing triangle with 8-deep dot products.  X is formed by back substitution with one thread per column
+// and 8-row panels (8 independent sums per panel), which needs no barrier.  The frame beyond nb is the identity.
 __device__ bool leaf_factor_invert(double* a, int lda, double* x, int ldx, int j0, int nb, DeviceStatus* st,
                                    double* smem) {
+  constexpr int P = 8;
   double(*U)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(smem);
   double(*X)[NB + 1] = U + NB;
   double* dinv = reinterpret_cast<double*>(X + NB);
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;  // 16 x 8 thread tile
-  __syncthreads();  // the block may just have been written by this CTA's other threads (the look-ahead tile update)
-  for (int idx = tid; idx < NB * NB; idx += kThreads) {  // the whole 64 x 64 frame: zero outside the block
-    const int r = idx % NB, c = idx / NB;
-    U[r][c] = (r <= c && c < nb) ? a[(j0 + r) + (size_t)(j0 + c) * lda] : 0.0;
-    X[r][c] = 0.0;
-  }
+  int* s_bad = reinterpret_cast<int*>(dinv + NB);
+  const int tid = threadIdx.x, lane = tid & 31;
   __syncthreads();
-  for (int k = 0; k < nb; ++k) {
-    const double piv = U[k][k];
-    if (!(piv > 0.0)) {
-      if (tid == 0) set_status(st, kStatusNotSPD, j0 + k + 1, 0);
-      __syncthreads();
-      return false;  // uniform: every thread read the same pivot
+  constexpr int kPer = NB * NB / kThreads / 2;
+  for (int pass = 0; pass < 2; ++pass) {
+    double v[kPer];
+#pragma unroll
+    for (int t = 0; t < kPer; ++t) {
+      const int idx = tid + kThreads * (pass * kPer + t), r = idx % NB, c = idx / NB;
+      v[t] = c < nb ? (r <= c ? a[(j0 + r) + (size_t)(j0 + c) * lda] : 0.0) : (r == c ? 1.0 : 0.0);
     }
-    const double inv = rsqrt(piv), u = piv * inv;  // one reciprocal square root on the step's critical path
-    const int c = k + 1 + tid;
-    if (c < nb) U[k][c] *= inv;
+#pragma unroll
+    for (int t = 0; t < kPer; ++t) {
+      const int idx = tid + kThreads * (pass * kPer + t), r = idx % NB, c = idx / NB;
+      U[r][c] = v[t];
+    }
+  }
+  if (tid == 0) *s_bad = -1;
+  const int tx = tid & 15, ty = tid >> 4;
+  for (int p0 = 0; p0 < NB; p0 += P) {
     __syncthreads();
-    for (int i = 0; i < 8; ++i) {
-      const int r = k + 1 + ty + 8 * i;
-      if (r >= nb) break;
-      const double ukr = U[k][r];
+    // (a) the 8 x 8 diagonal block by one warp: lane c (mod 8) holds its column.
+    if (tid < 32) {
+      const int c = lane & 7;
+      double d[P];
+#pragma unroll
+      for (int i = 0; i < P; ++i) d[i] = i <= c ? U[p0 + i][p0 + c] : 0.0;
+      int bad = -1;
+      double dv = 0.0;
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        const double piv = __shfl_sync(0xffffffffu, d[k], k, P);
+        if (!(piv > 0.0) && bad < 0) bad = k;
+        const double inv = rsqrt(piv);
+        const double ukc = d[k] * inv;
+        if (c == k) dv = inv;
+#pragma unroll
+        for (int i = k + 1; i < P; ++i) {
+          const double uki = __shfl_sync(0xffffffffu, ukc, i, P);
+          if (i <= c) d[i] = fma(-uki, ukc, d[i]);
+        }
+        d[k] = ukc;
+      }
+      if (lane < P) {
+#pragma unroll
+        for (int i = 0; i < P; ++i)
+          if (i <= c) U[p0 + i][p0 + c] = d[i];
+        dinv[p0 + c] = dv;
+        if (lane == 0 && bad >= 0) *s_bad = p0 + bad;
+      }
+    }
+    __syncthreads();
+    if (*s_bad >= 0) {
+      if (tid == 0) set_status(st, kStatusNotSPD, j0 + *s_bad + 1, 0);
+      __syncthreads();
+      return false;
+    }
+    // (b) the panel's block row: U(p0:p0+8, c) = U_d^-T A(p0:p0+8, c), one thread per column.
+    {
+      const int c = p0 + P + tid;
+      if (c < NB) {
+        double u[P];
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          double s = U[p0 + q][c];
+#pragma unroll
+          for (int pp = 0; pp < q; ++pp) s = fma(-U[p0 + pp][p0 + q], u[pp], s);
+          u[q] = s * dinv[p0 + q];
+        }
+#pragma unroll
+        for (int q = 0; q < P; ++q) U[p0 + q][c] = u[q];
+      }
+    }
+    __syncthreads();
+    // (c) trailing update A(r, c) -= sum_q U(p0+q, r) U(p0+q, c), r <= c in [p0+8, 64).
+    {
+      const int b = p0 + P;
+      double uc[4][P];
 #pragma unroll
       for (int jj = 0; jj < 4; ++jj) {
-        const int cc = k + 1 + tx + 16 * jj;
-        if (cc >= r && cc < nb) U[r][cc] -= ukr * U[k][cc];
+        const int c = b + tx + 16 * jj;
+#pragma unroll
+        for (int q = 0; q < P; ++q) uc[jj][q] = c < NB ? U[p0 + q][c] : 0.0;
       }
-    }
-    if (tid == 0) {
-      U[k][k] = u;  // nobody reads U(k,k) after this step's pivot read
-      dinv[k] = inv;
-    }
-    __syncthreads();
-  }
-  for (int idx = tid; idx < nb * nb; idx += kThreads) {
-    const int r = idx % nb, c = idx / nb;
-    if (r <= c) a[(j0 + r) + (size_t)(j0 + c) * lda] = U[r][c];
-  }
-  // Inverse by doubling inside the block: 8 x 8 diagonal blocks by back substitution (one thread per column), then
-  // joins of neighbouring blocks for sizes 8, 16, 32: T = U12 X22 (kept transposed in U's unused strict lower part),
-  // X12 = -X11 T.  The frame beyond nb is zero, so the joins can run over the full 64 x 64 frame.
-  if (tid < NB) {
-    const int c = tid, b0 = (c / 8) * 8;
-    if (c < nb) {
-      X[c][c] = dinv[c];
-      for (int i = c - 1; i >= b0; --i) {
-        double sacc = 0.0;
-        for (int q = i + 1; q <= c; ++q) sacc += U[i][q] * X[q][c];
-        X[i][c] = -dinv[i] * sacc;
+      for (int i = 0; i < 8; ++i) {
+        const int r = b + ty + 8 * i;
+        if (r >= NB) break;
+        double ur[P];
+#pragma unroll
+        for (int q = 0; q < P; ++q) ur[q] = U[p0 + q][r];
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const int c = b + tx + 16 * jj;
+          if (c >= r && c < NB) {
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int q = 0; q < P; q += 2) {
+              s0 = fma(ur[q], uc[jj][q], s0);
+              s1 = fma(ur[q + 1], uc[jj][q + 1], s1);
+            }
+            U[r][c] -= s0 + s1;
+          }
+        }
       }
     }
   }
   __syncthreads();
-  for (int sz = 8; sz < NB; sz *= 2) {
-    const int npair = NB / (2 * sz);
-    for (int idx = tid; idx < npair * sz * sz; idx += kThreads) {
-      const int pr = idx / (sz * sz), rem = idx % (sz * sz);
-      const int r = pr * 2 * sz + rem % sz, c = pr * 2 * sz + sz + rem / sz;
-      double sacc = 0.0;
-      for (int q = pr * 2 * sz + sz; q <= c; ++q) sacc += U[r][q] * X[q][c];
-      U[c][r] = sacc;
+  // X = U^-1 by columns (one thread each), 8-row panels upward: beyond-panel sums with 8 accumulators, then the
+  // panel's own 8 x 8 back substitution.
+  if (tid < NB) {
+    const int c = tid;
+    for (int i0 = (c / P) * P; i0 >= 0; i0 -= P) {
+      double s[P];
+#pragma unroll
+      for (int ii = 0; ii < P; ++ii) s[ii] = 0.0;
+      for (int q = i0 + P; q <= c; ++q) {
+        const double xq = X[q][c];
+#pragma unroll
+        for (int ii = 0; ii < P; ++ii) s[ii] = fma(U[i0 + ii][q], xq, s[ii]);
+      }
+      double xv[P];
+#pragma unroll
+      for (int ii = P - 1; ii >= 0; --ii) {
+        const int r = i0 + ii;
+        double t = s[ii];
+#pragma unroll
+        for (int jj = ii + 1; jj < P; ++jj) t = fma(U[r][i0 + jj], xv[jj], t);
+        xv[ii] = r > c ? 0.0 : (r == c ? dinv[c] : -dinv[r] * t);
+      }
+#pragma unroll
+      for (int ii = 0; ii < P; ++ii) X[i0 + ii][c] = xv[ii];
     }
-    __syncthreads();
-    for (int idx = tid; idx < npair * sz * sz; idx += kThreads) {
-      const int pr = idx / (sz * sz), rem = idx % (sz * sz);
-      const int r = pr * 2 * sz + rem % sz, c = pr * 2 * sz + sz + rem / sz;
-      double sacc = 0.0;
-      const int qe = pr * 2 * sz + sz;
-      for (int q = r; q < qe; ++q) sacc += X[r][q] * U[c][q];
-      X[r][c] = -sacc;
-    }
-    __syncthreads();
+    for (int r = (c / P) * P + P; r < NB; ++r) X[r][c] = 0.0;
   }
-  for (int idx = tid; idx < nb * nb; idx += kThreads) {
-    const int r = idx % nb, c = idx / nb;
-    x[(j0 + r) + (size_t)(j0 + c) * ldx] = X[r][c];
+  __syncthreads();
+  for (int idx = tid; idx < NB * NB; idx += kThreads) {
+    const int r = idx % NB, c = idx / NB;
+    if (r <= c && c < nb) {
+      a[(j0 + r) + (size_t)(j0 + c) * lda] = U[r][c];
+      x[(j0 + r) + (size_t)(j0 + c) * ldx] = X[r][c];
+    }
   }
   __syncthreads();
   return true;
 }
+
 
 __device__ __forceinline__ GemmDesc<double> tile_desc(int M, int N, int K, double alpha, const double* A, int lda,
                                                       int transA, const double* B, int ldb, double beta, double* C,
