@@ -104,7 +104,8 @@ int xtb_dsygvd_factored_device(int n, double* a, int lda, const double* u, int l
  * SCC cycle's C), w receives the eigenvalues.  `iters` Ogita-Aishima steps in the S inner product (the reference's refinement,
  * scripts/kernels/refine.f90:258-325, with S in place of the identity; clusters of eigenvalues closer than delta =
  * clamp(32 max|C^T H C|_offdiag, 1e-10, 1e-3) solved exactly within their block), then c, w in ascending order.
- * Returns 0, -1000 - cudaError, or -(argument position) for an invalid argument (iters in 1..10). */
+ * Its GEMMs run on the FP64 engine of the solve plan ("dgemm_engine").  Returns 0, -1000 - cudaError, or -(argument
+ * position) for an invalid argument (iters in 1..10). */
 int xtb_dsygvd_refine_device(int n, const double* h, int ldh, const double* s, int lds, double* c, int ldc,
                              double* w, int iters, void* stream);
 

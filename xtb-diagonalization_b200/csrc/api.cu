@@ -1245,14 +1245,17 @@ int xtb_dsygvd_refine_device(int n, const double* h, int ldh, const double* s, i
   if (n == 0) return 0;
   Context* c0 = context();
   if (!c0) return t_state.last_code;
+  t_plan = plan_for(n, 64);
   Call k(c0, (cudaStream_t)stream, true);
   double* hf = k.dev<double>("rf.H", (size_t)n * n);
   double* sf = k.dev<double>("rf.S", (size_t)n * n);
   double* rw = k.dev<double>("mx.refine", refine_work_elems(n));
+  TcGemm tc = tc_engine(k, n);
+  tc.passes = 0;  // every update FP64: the GEMMs run on the plan's FP64 engine
   if (k.ok()) {
     symmetrize_upper<double>(n, h, ldh, hf, n, k.s);
     symmetrize_upper<double>(n, s, lds, sf, n, k.s);
-    k.check(refine_generalized(n, hf, n, sf, n, nullptr, 0, c, ldc, w, iters, rw, c0->arena, k.s), "refine");
+    k.check(refine_generalized(n, hf, n, sf, n, nullptr, 0, c, ldc, w, iters, rw, c0->arena, k.s, &tc), "refine");
   }
   DeviceStatus st{};
   const int code = k.finish(&st);
