@@ -810,6 +810,10 @@ def run_ours(args):
                                     f"generalized eigensolve n={n} seed={args.seed}") + ", all eigenpairs, FP64 path",
                        "eigenvalue_reference": eig_reference,
                        "path": "potrf, trtri, X^T H X, resident sytrd, D&C stedc, WY ormtr, X C' (all CUDA)",
+                       "fp64_gemm_engine": ("int8 Ozaki splitting on tcgen05 for GEMMs >= 512^3 (exact int32 slice "
+                                            "products, one FP64 rounding; FP64 accuracy), DMMA below"
+                                            if (plans["fp64"]["dgemm"] if plans else
+                                                xtbeig.get_option("dgemm_engine")) else "FP64 DMMA"),
                        "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}",
                        "eigenvalue_error_vs_exact": eig_err, "wall_s_timed_region": round(t_wall, 3)},
             "roofline": {"bound": "hbm", "kernel": "sytrd_resident_kernel",
