@@ -504,6 +504,16 @@ TcGemm tc_engine(Call& k, int n) {
   return tc;
 }
 
+// tc_engine plus the refinement's sliced-operand workspace (used only by the stages that refine).
+TcGemm tc_engine_refine(Call& k, int n) {
+  TcGemm tc = tc_engine(k, n);
+  if (tc.oz_work) {
+    tc.oz_ops_bytes = refine_ozaki_bytes(n);
+    tc.oz_ops = k.template dev<char>("ozaki.ops", tc.oz_ops_bytes);
+  }
+  return tc;
+}
+
 void stage_stedc(Call& k, int n, double* d, double* e, double* z, int ldz) {
   if (!k.ok() || n <= 0) return;
   const size_t wb = stedc_work_bytes(n);
@@ -581,7 +591,7 @@ void solve_factored_mixed(Call& k, int n, double* h, const double* u, int ldu, c
   float* zf = rf + nn;
   float* df = zf + nn;
   float* ef = df + n;
-  const TcGemm tc = tc_engine(k, n);
+  const TcGemm tc = tc_engine_refine(k, n);
   if (!k.ok()) return;
   convert_mat_f64_to_f32(n, n, x, ldx, xf, n, k.s);
   convert_mat_f64_to_f32(n, n, h, n, hf, n, k.s);
@@ -1250,7 +1260,7 @@ int xtb_dsygvd_refine_device(int n, const double* h, int ldh, const double* s, i
   double* hf = k.dev<double>("rf.H", (size_t)n * n);
   double* sf = k.dev<double>("rf.S", (size_t)n * n);
   double* rw = k.dev<double>("mx.refine", refine_work_elems(n));
-  TcGemm tc = tc_engine(k, n);
+  TcGemm tc = tc_engine_refine(k, n);
   tc.passes = 0;  // every update FP64: the GEMMs run on the plan's FP64 engine
   if (k.ok()) {
     symmetrize_upper<double>(n, h, ldh, hf, n, k.s);

@@ -91,6 +91,23 @@ inline size_t tc_work_elems(int n) { return 6 * (size_t)(n + 64) * (size_t)(n + 
 size_t ozaki_work_bytes(int M, int N, int K);
 cudaError_t ozaki_dgemm(const GemmDesc<double>& p, void* work, size_t work_bytes, DeviceStatus* st, uint64_t limit_ns,
                         cudaStream_t s);
+// The same engine on operands sliced once and used in several products (the same slices and scales give the same
+// result bit for bit as ozaki_dgemm).  An operand is R rows of K elements, element (r, k) at X[r sr + k sk]: op(A)'s
+// rows, or op(B)'s columns; keep 1 zeroes k < r, keep 2 zeroes k > r (triangular operands).  ozaki_gemm_sliced forms
+// C = alpha a b^T + beta C (a: M rows, b: N rows, the same K); mode's kTri* flags clip the K range like the slicing's
+// keep, kCUpper skips the tiles below the diagonal.
+struct OzSliced {
+  int8_t* slices = nullptr;               // 8 x R x Kp
+  unsigned long long* maxbits = nullptr;  // R: the rows' largest |x|
+  int R = 0, K = 0;
+};
+size_t ozaki_operand_bytes(int R, int K);
+size_t ozaki_product_bytes(int M, int N);
+cudaError_t ozaki_slice(const double* X, long long sr, long long sk, int R, int K, int keep, void* mem, size_t bytes,
+                        OzSliced* out, cudaStream_t s);
+cudaError_t ozaki_gemm_sliced(const OzSliced& a, const OzSliced& b, double alpha, double beta, double* C, int ldc,
+                              int mode, void* work, size_t work_bytes, DeviceStatus* st, uint64_t limit_ns,
+                              cudaStream_t s);
 
 struct DescArena;
 // Which engine runs a stage's GEMMs.  FP32 problems: passes 0 = the grouped GEMM on the CUDA cores, 1 or 3 = the
@@ -103,6 +120,8 @@ struct TcGemm {
   int dgemm = 0;
   void* oz_work = nullptr;
   size_t oz_bytes = 0;
+  void* oz_ops = nullptr;  // the refinement's sliced operands and product scratch (refine_ozaki_bytes), may be NULL
+  size_t oz_ops_bytes = 0;
   DeviceStatus* st = nullptr;
   uint64_t limit_ns = 0;
 };
@@ -208,6 +227,8 @@ cudaError_t dk_adjoint(int n, const double* c, const double* e, double mu, doubl
 // FP64 Ogita-Aishima refinement of C (n x n, ldc) for H C = S C diag(w), C^T S C = I: `iters` steps, then c and w
 // rewritten in ascending eigenvalue order.  h, s full symmetric (FP64).  work: refine_work_elems(n) doubles.
 size_t refine_work_elems(int n);
+// Bytes of TcGemm::oz_ops that lets the refinement slice each operand once (H, S or U once per call).
+size_t refine_ozaki_bytes(int n);
 // u (may be NULL): the upper Cholesky factor of s (ld ldu); with it C^T S C is formed as (U C)^T (U C).
 // tc (may be NULL): with a tensor-core engine, every step's update C (I + E) but the last runs as C D (the clusters'
 // blocks, FP64) + C F (the first-order remainder, on the tensor cores); the last update stays FP64.  tc->dgemm

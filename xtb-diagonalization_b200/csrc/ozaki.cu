@@ -460,7 +460,111 @@ inline size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
 
 bool g_oz_smem[64];
 
+// The pairs and finish launches of C = alpha a b^T + beta C for two sliced operands (a: M rows of K, b: N rows of K).
+// T and U are M x N scratch (ld M); counter must be zero.
+cudaError_t oz_product(const OzSliced& a, const OzSliced& b, double alpha, double beta, double* C, int ldc, int mode,
+                       double* T, double* U, unsigned* counter, DeviceStatus* st, uint64_t limit_ns, cudaStream_t s) {
+  const int M = a.R, N = b.R, K = a.K, Kp = oz_kp(K);
+  cudaError_t err;
+  if (K > 0) {
+    OzParams Q;
+    memset(&Q, 0, sizeof(Q));
+    if (!oz_encode(&Q.a, a.slices, kOzS * M, Kp) || !oz_encode(&Q.b, b.slices, kOzS * N, Kp))
+      return cudaErrorInvalidValue;
+    Q.T = T;
+    Q.U = U;
+    Q.M = M;
+    Q.N = N;
+    Q.K = K;
+    Q.mode = mode;
+    Q.tiles_m = (M + kOBM - 1) / kOBM;
+    Q.tiles = Q.tiles_m * ((N + kOBN - 1) / kOBN);
+    Q.counter = counter;
+    Q.st = st;
+    Q.limit_ns = limit_ns;
+    int dev = 0, sms = 0;
+    if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
+    if ((err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return err;
+    if (dev < 0 || dev >= 64 || !g_oz_smem[dev]) {
+      err = cudaFuncSetAttribute(oz_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOSmemBytes);
+      if (err != cudaSuccess) return err;
+      if (dev >= 0 && dev < 64) g_oz_smem[dev] = true;
+    }
+    oz_pairs_kernel<<<std::min(2 * Q.tiles, sms), kOThreads, kOSmemBytes, s>>>(Q);
+    note_launches();
+  }
+  OzFinish F;
+  F.T = T;
+  F.U = U;
+  F.maxa = a.maxbits;
+  F.maxb = b.maxbits;
+  F.C = C;
+  F.ldc = ldc;
+  F.M = M;
+  F.N = N;
+  F.mode = mode;
+  F.have_k = K > 0;
+  F.alpha = alpha;
+  F.beta = beta;
+  oz_finish_kernel<<<dim3((M + 255) / 256, std::min(N, 65535)), 256, 0, s>>>(F);
+  note_launches();
+  return cudaGetLastError();
+}
+
 }  // namespace
+
+size_t ozaki_operand_bytes(int R, int K) {
+  return up256((size_t)kOzS * std::max(R, 1) * oz_kp(K)) + up256((size_t)std::max(R, 1) * 8) + 256;
+}
+
+size_t ozaki_product_bytes(int M, int N) { return 2 * up256((size_t)M * N * 8) + 512; }
+
+cudaError_t ozaki_slice(const double* X, long long sr, long long sk, int R, int K, int keep, void* mem, size_t bytes,
+                        OzSliced* out, cudaStream_t s) {
+  if (R <= 0 || K < 0 || K > kOzMaxK || ozaki_operand_bytes(R, K) > bytes) return cudaErrorInvalidValue;
+  const int Kp = oz_kp(K);
+  char* w = reinterpret_cast<char*>(((uintptr_t)mem + 255) & ~uintptr_t(255));
+  out->slices = reinterpret_cast<int8_t*>(w);
+  w += up256((size_t)kOzS * R * Kp);
+  out->maxbits = reinterpret_cast<unsigned long long*>(w);
+  out->R = R;
+  out->K = K;
+  cudaError_t err = cudaMemsetAsync(out->maxbits, 0, (size_t)R * 8, s);
+  if (err != cudaSuccess || K == 0) return err;
+  OzPrep P;
+  memset(&P, 0, sizeof(P));
+  OzOperand& o = P.op[0];
+  o.X = X;
+  o.sr = sr;
+  o.sk = sk;
+  o.R = R;
+  o.keep = keep;
+  o.maxbits = out->maxbits;
+  o.slices = out->slices;
+  P.K = K;
+  P.Kp = Kp;
+  const dim3 grid((R + kOTile - 1) / kOTile, Kp / kOTile, 1);
+  oz_max_kernel<<<grid, 256, 0, s>>>(P);
+  oz_slice_kernel<<<grid, 256, 0, s>>>(P);
+  note_launches(2);
+  return cudaGetLastError();
+}
+
+cudaError_t ozaki_gemm_sliced(const OzSliced& a, const OzSliced& b, double alpha, double beta, double* C, int ldc,
+                              int mode, void* work, size_t work_bytes, DeviceStatus* st, uint64_t limit_ns,
+                              cudaStream_t s) {
+  if (a.R <= 0 || b.R <= 0) return cudaSuccess;
+  if (a.K != b.K || ozaki_product_bytes(a.R, b.R) > work_bytes) return cudaErrorInvalidValue;
+  char* w = reinterpret_cast<char*>(((uintptr_t)work + 255) & ~uintptr_t(255));
+  double* T = reinterpret_cast<double*>(w);
+  w += up256((size_t)a.R * b.R * 8);
+  double* U = reinterpret_cast<double*>(w);
+  w += up256((size_t)a.R * b.R * 8);
+  unsigned* counter = reinterpret_cast<unsigned*>(w);
+  const cudaError_t err = cudaMemsetAsync(counter, 0, sizeof(unsigned), s);
+  if (err != cudaSuccess) return err;
+  return oz_product(a, b, alpha, beta, C, ldc, mode, T, U, counter, st, limit_ns, s);
+}
 
 size_t ozaki_work_bytes(int M, int N, int K) {
   const size_t kp = (size_t)oz_kp(K);
@@ -512,48 +616,9 @@ cudaError_t ozaki_dgemm(const GemmDesc<double>& p, void* work, size_t work_bytes
     oz_max_kernel<<<grid, 256, 0, s>>>(P);
     oz_slice_kernel<<<grid, 256, 0, s>>>(P);
     note_launches(2);
-
-    OzParams Q;
-    memset(&Q, 0, sizeof(Q));
-    if (!oz_encode(&Q.a, sa, kOzS * p.M, Kp) || !oz_encode(&Q.b, sb, kOzS * p.N, Kp)) return cudaErrorInvalidValue;
-    Q.T = T;
-    Q.U = U;
-    Q.M = p.M;
-    Q.N = p.N;
-    Q.K = K;
-    Q.mode = p.mode;
-    Q.tiles_m = (p.M + kOBM - 1) / kOBM;
-    Q.tiles = Q.tiles_m * ((p.N + kOBN - 1) / kOBN);
-    Q.counter = counter;
-    Q.st = st;
-    Q.limit_ns = limit_ns;
-    int dev = 0, sms = 0;
-    if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
-    if ((err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return err;
-    if (dev < 0 || dev >= 64 || !g_oz_smem[dev]) {
-      err = cudaFuncSetAttribute(oz_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOSmemBytes);
-      if (err != cudaSuccess) return err;
-      if (dev >= 0 && dev < 64) g_oz_smem[dev] = true;
-    }
-    oz_pairs_kernel<<<std::min(2 * Q.tiles, sms), kOThreads, kOSmemBytes, s>>>(Q);
-    note_launches();
   }
-  OzFinish F;
-  F.T = T;
-  F.U = U;
-  F.maxa = maxbits;
-  F.maxb = maxbits + p.M;
-  F.C = p.C;
-  F.ldc = p.ldc;
-  F.M = p.M;
-  F.N = p.N;
-  F.mode = p.mode;
-  F.have_k = K > 0;
-  F.alpha = p.alpha;
-  F.beta = p.beta;
-  oz_finish_kernel<<<dim3((p.M + 255) / 256, std::min(p.N, 65535)), 256, 0, s>>>(F);
-  note_launches();
-  return cudaGetLastError();
+  OzSliced oa{sa, maxbits, p.M, K}, ob{sb, maxbits + p.M, p.N, K};
+  return oz_product(oa, ob, p.alpha, p.beta, p.C, p.ldc, p.mode, T, U, counter, st, limit_ns, s);
 }
 
 }  // namespace xtbeig

@@ -345,6 +345,9 @@ __global__ void scatter_columns_kernel(int n, const double* __restrict__ src, in
 // for the tensor-core update.
 size_t refine_work_elems(int n) { return (size_t)7 * n * n + 6 * (size_t)n + 160 + ((size_t)3 * n * n + 1) / 2; }
 
+// Seven sliced operands (H, S or U, C by columns, H C, U C or S C, C by rows, M) and one product's scratch.
+size_t refine_ozaki_bytes(int n) { return 7 * ozaki_operand_bytes(n, n) + ozaki_product_bytes(n, n); }
+
 cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s, int lds, const double* u, int ldu,
                                double* c, int ldc, double* w, int iters, double* work, DescArena& arena,
                                cudaStream_t st, const TcGemm* tc) {
@@ -370,24 +373,61 @@ cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s,
   TcGemm tc64;  // the FP64 GEMMs: the engine the caller chose (DMMA without one)
   if (tc) tc64 = *tc;
   tc64.passes = 0;
+  // On the Ozaki engine with room for the sliced operands, every operand is sliced once and reused: H and S (or U)
+  // once per call; C by columns serves H C, U C (or S C) and C^T (H C); U C by columns serves both sides of
+  // (U C)^T (U C).  The products are the ones ozaki_dgemm would form, bit for bit.
+  const bool oz = tc64.dgemm == 1 && tc64.oz_ops && tc64.oz_ops_bytes >= refine_ozaki_bytes(n) &&
+                  ozaki_eligible(n, n, n);
+  OzSliced Hs, Ss, Cs, Ys, Zs, Cr, Ms;
+  char* ozp = nullptr;
+  size_t opb = 0;
+  void* prod = nullptr;
+  size_t prodb = 0;
+  auto oz_mem = [&](int i) { return static_cast<void*>(ozp + (size_t)i * opb); };
+  if (oz) {
+    ozp = static_cast<char*>(tc64.oz_ops);
+    opb = ozaki_operand_bytes(n, n);
+    prod = ozp + 7 * opb;
+    prodb = tc64.oz_ops_bytes - 7 * opb;
+  }
+  cudaError_t err = cudaSuccess;
+  auto product = [&](const OzSliced& a, const OzSliced& b, double* out, int mode) {
+    return ozaki_gemm_sliced(a, b, 1.0, 0.0, out, n, mode, prod, prodb, tc64.st, tc64.limit_ns, st);
+  };
+  if (oz) {
+    if ((err = ozaki_slice(h, 1, ldh, n, n, 0, oz_mem(0), opb, &Hs, st)) != cudaSuccess) return err;
+    err = u ? ozaki_slice(u, 1, ldu, n, n, 1, oz_mem(1), opb, &Ss, st)
+            : ozaki_slice(s, 1, lds, n, n, 0, oz_mem(1), opb, &Ss, st);
+    if (err != cudaSuccess) return err;
+  }
   // The current iterate alternates between cur and nxt; the result is scattered into c in ascending order.
   const double* cur = c;
   int ldcur = ldc;
   double* nxt = c2;
-  cudaError_t err = cudaSuccess;
   if (iters < 1) iters = 1;
   for (int it = 0; it < iters; ++it) {
     GemmDesc<double> p[2];
     // A = C^T (H C); B = C^T S C, as (U C)^T (U C) when the Cholesky factor U of S is given (2 n^3 flops instead
     // of 3 n^3: U C is triangular times full).
-    p[0] = gemm_problem<double>(n, n, n, 1.0, h, ldh, 0, cur, ldcur, 0, 0.0, t1, n);
-    p[1] = u ? gemm_problem<double>(n, n, n, 1.0, u, ldu, 0, cur, ldcur, 0, 0.0, t2, n, kTriAUpper)
-             : gemm_problem<double>(n, n, n, 1.0, s, lds, 0, cur, ldcur, 0, 0.0, t2, n);
-    if ((err = gemm_run(arena, tc64, p, 2, st)) != cudaSuccess) return err;
-    p[0] = gemm_problem<double>(n, n, n, 1.0, cur, ldcur, 1, t1, n, 0, 0.0, A, n, kCUpper);
-    p[1] = u ? gemm_problem<double>(n, n, n, 1.0, t2, n, 1, t2, n, 0, 0.0, B, n, kCUpper)
-             : gemm_problem<double>(n, n, n, 1.0, cur, ldcur, 1, t2, n, 0, 0.0, B, n, kCUpper);
-    if ((err = gemm_run(arena, tc64, p, 2, st)) != cudaSuccess) return err;
+    if (oz) {
+      if ((err = ozaki_slice(cur, ldcur, 1, n, n, 0, oz_mem(2), opb, &Cs, st)) != cudaSuccess ||
+          (err = product(Hs, Cs, t1, 0)) != cudaSuccess ||
+          (err = product(Ss, Cs, t2, u ? kTriAUpper : 0)) != cudaSuccess ||
+          (err = ozaki_slice(t1, n, 1, n, n, 0, oz_mem(3), opb, &Ys, st)) != cudaSuccess ||
+          (err = product(Cs, Ys, A, kCUpper)) != cudaSuccess ||
+          (err = ozaki_slice(t2, n, 1, n, n, 0, oz_mem(4), opb, &Zs, st)) != cudaSuccess ||
+          (err = product(u ? Zs : Cs, Zs, B, kCUpper)) != cudaSuccess)
+        return err;
+    } else {
+      p[0] = gemm_problem<double>(n, n, n, 1.0, h, ldh, 0, cur, ldcur, 0, 0.0, t1, n);
+      p[1] = u ? gemm_problem<double>(n, n, n, 1.0, u, ldu, 0, cur, ldcur, 0, 0.0, t2, n, kTriAUpper)
+               : gemm_problem<double>(n, n, n, 1.0, s, lds, 0, cur, ldcur, 0, 0.0, t2, n);
+      if ((err = gemm_run(arena, tc64, p, 2, st)) != cudaSuccess) return err;
+      p[0] = gemm_problem<double>(n, n, n, 1.0, cur, ldcur, 1, t1, n, 0, 0.0, A, n, kCUpper);
+      p[1] = u ? gemm_problem<double>(n, n, n, 1.0, t2, n, 1, t2, n, 0, 0.0, B, n, kCUpper)
+               : gemm_problem<double>(n, n, n, 1.0, cur, ldcur, 1, t2, n, 0, 0.0, B, n, kCUpper);
+      if ((err = gemm_run(arena, tc64, p, 2, st)) != cudaSuccess) return err;
+    }
     mirror_upper_inplace<double>(n, A, n, st);
     mirror_upper_inplace<double>(n, B, n, st);
     if ((err = cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), st)) != cudaSuccess) return err;
@@ -398,8 +438,15 @@ cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s,
     // The tensor-core update only where a later step corrects its error (about 2e-5 relative to the correction, from
     // the tensor cores' FP32 accumulation); the last step's update stays FP64, which sets the final accuracy.
     if (!tc_update || it == iters - 1) {
-      p[0] = gemm_problem<double>(n, n, n, 1.0, cur, ldcur, 0, M, n, 0, 0.0, nxt, n);
-      if ((err = gemm_run(arena, tc64, p, 1, st)) != cudaSuccess) return err;
+      if (oz) {
+        if ((err = ozaki_slice(cur, 1, ldcur, n, n, 0, oz_mem(5), opb, &Cr, st)) != cudaSuccess ||
+            (err = ozaki_slice(M, n, 1, n, n, 0, oz_mem(6), opb, &Ms, st)) != cudaSuccess ||
+            (err = product(Cr, Ms, nxt, 0)) != cudaSuccess)
+          return err;
+      } else {
+        p[0] = gemm_problem<double>(n, n, n, 1.0, cur, ldcur, 0, M, n, 0, 0.0, nxt, n);
+        if ((err = gemm_run(arena, tc64, p, 1, st)) != cudaSuccess) return err;
+      }
     } else {
       // nxt = C M = C D + C F: the clusters' rotations in FP64, the small first-order remainder F on the tensor
       // cores.
