@@ -8,8 +8,8 @@
 // its time in launch and pipeline-fill latency).  Blocks of 64 columns, right-looking, with grid barriers:
 //   step j:  B  all CTAs: block row U(j, j+1:) = X(j,j)^T A(j, j+1:)       (64 x 64 DMMA tiles, in place)
 //            --- barrier ---
-//            C  CTA 0: tile (j+1, j+1) of the trailing update, then factors and inverts that diagonal block in shared
-//               memory (look-ahead: the next step's diagonal work overlaps the rest of the update);
+//            C  CTA 0: tile (j+1, j+1) of the trailing update, then factors and inverts that diagonal block, all in
+//               shared memory (look-ahead: the next step's diagonal work overlaps the rest of the update);
 //               other CTAs: the remaining upper tiles of A(j+1:, j+1:) -= U(j, j+1:)^T U(j, j+1:)
 //            --- barrier ---
 // then X by doubling over block sizes 64, 128, ...: X12 = -X11 (U12 X22), every tile of a level in parallel.
@@ -49,8 +49,11 @@ constexpr size_t kSmemBytes = (tile::smem_elems<double>() + kLeafElems) * sizeof
 // diagonal block by one warp with shuffles, its block row by a triangular solve per column, then the rank-8 update
 // of the trailing triangle with 8-deep dot products.  X is formed by back substitution with one thread per column
 // and 8-row panels (8 independent sums per panel), which needs no barrier.  The frame beyond nb is the identity.
-__device__ bool leaf_factor_invert(double* a, int lda, double* x, int ldx, int j0, int nb, DeviceStatus* st,
-                                   double* smem) {
+// With a panel (the kp x nb block row U(j0 - kp : j0, j0 : j0 + nb), ld lda), the block's trailing update
+// A -= P^T P runs first, in shared memory with 8 x 4 register tiles per thread (gsm: the tile pipeline's region,
+// free while the leaf runs, holds P).
+__device__ bool leaf_factor_invert(const double* panel, int kp, double* a, int lda, double* x, int ldx, int j0,
+                                   int nb, DeviceStatus* st, double* smem, double* gsm) {
   constexpr int P = 8;
   double(*U)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(smem);
   double(*X)[NB + 1] = U + NB;
@@ -73,6 +76,49 @@ __device__ bool leaf_factor_invert(double* a, int lda, double* x, int ldx, int j
     }
   }
   if (tid == 0) *s_bad = -1;
+  if (panel) {
+    double(*Pn)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(gsm);
+    for (int pass = 0; pass < 2; ++pass) {
+      double v[kPer];
+#pragma unroll
+      for (int t = 0; t < kPer; ++t) {
+        const int idx = tid + kThreads * (pass * kPer + t), r = idx % NB, c = idx / NB;
+        v[t] = (r < kp && c < nb) ? panel[r + (size_t)c * lda] : 0.0;
+      }
+#pragma unroll
+      for (int t = 0; t < kPer; ++t) {
+        const int idx = tid + kThreads * (pass * kPer + t);
+        Pn[idx % NB][idx / NB] = v[t];
+      }
+    }
+    __syncthreads();
+    // Thread (rb, cb) owns rows rb + 8 i and columns cb + 16 j (i < 8, j < 4): the 8 lanes of a row group read
+    // consecutive panel entries, the column reads are broadcasts.
+    const int rb = tid & 7, cb = tid >> 3;
+    double acc[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int k = 0; k < kp; ++k) {
+      double pr[8], pc[4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) pr[i] = Pn[k][rb + 8 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) pc[j] = Pn[k][cb + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(pr[i], pc[j], acc[i][j]);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int r = rb + 8 * i, c = cb + 16 * j;
+        if (r <= c && c < nb) U[r][c] -= acc[i][j];
+      }
+  }
   const int tx = tid & 15, ty = tid >> 4;
   for (int p0 = 0; p0 < NB; p0 += P) {
     __syncthreads();
@@ -228,7 +274,7 @@ __global__ void __launch_bounds__(kThreads, 1) potrf_persistent_kernel(PotrfPara
   if (ld_volatile_i32(&p.st->code) != 0) return;
   auto bsize = [&](int b) { return min(NB, n - b * NB); };
 
-  if (cta == 0) leaf_factor_invert(a, lda, x, ldx, 0, bsize(0), p.st, lsm);
+  if (cta == 0) leaf_factor_invert(nullptr, 0, a, lda, x, ldx, 0, bsize(0), p.st, lsm, gsm);
   if (!group_barrier(p.counter, (unsigned)G, epoch, p.st, p.limit_ns)) return;
   if (ld_volatile_i32(&p.st->code) != 0) return;
 
@@ -246,10 +292,7 @@ __global__ void __launch_bounds__(kThreads, 1) potrf_persistent_kernel(PotrfPara
     const int m = nt - j - 1;
     if (cta == 0) {
       const int r0 = (j + 1) * NB;
-      GemmDesc<double> d = tile_desc(bsize(j + 1), bsize(j + 1), nbj, -1.0, a + j0 + (size_t)r0 * lda, lda, 1,
-                                     a + j0 + (size_t)r0 * lda, lda, 1.0, a + r0 + (size_t)r0 * lda, lda, kCUpper);
-      tile::gemm_tile<double>(d, 0, 0, gsm);
-      leaf_factor_invert(a, lda, x, ldx, r0, bsize(j + 1), p.st, lsm);
+      leaf_factor_invert(a + j0 + (size_t)r0 * lda, nbj, a, lda, x, ldx, r0, bsize(j + 1), p.st, lsm, gsm);
     }
     const int ntile = m * (m + 1) / 2 - 1;  // upper tiles of the m x m trailing block, except (j+1, j+1)
     const int workers = G > 1 ? G - 1 : 1;
