@@ -244,7 +244,8 @@ def dsygvd_factored_device(n, a_ptr, lda, u_ptr, ldu, x_ptr, ldx, w_ptr, stream=
 
 
 def dgemm_device(transa, transb, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc, stream=0) -> int:
-    """xtb_dgemm_device: FP64 GEMM on the FP64 tensor cores on device pointers."""
+    """xtb_dgemm_device: FP64 GEMM on device pointers (option "dgemm_engine": 0 DMMA, 1 int8 Ozaki from 512^3 up, the
+    default, 2 Ozaki at every size)."""
     return lib().xtb_dgemm_device(transa, transb, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc, stream)
 
 
