@@ -101,6 +101,14 @@ __device__ __forceinline__ bool group_barrier(unsigned* counter, unsigned member
   return s_ok != 0;
 }
 
+// The arrival half of group_barrier: the CTA counts itself in (release: its earlier writes are visible to whoever
+// waits on the barrier) and goes on without waiting.  The next group_barrier it calls waits for this epoch too.
+__device__ __forceinline__ void group_arrive(unsigned* counter, unsigned& epoch) {
+  __syncthreads();
+  epoch += 1;
+  if (threadIdx.x == 0) red_release_add_u32(counter, 1u);
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

@@ -287,7 +287,13 @@ __global__ void __launch_bounds__(kThreads, 1) potrf_persistent_kernel(PotrfPara
                                      a + j0 + (size_t)c0 * lda, lda, 0.0, a + j0 + (size_t)c0 * lda, lda, kTriALower);
       tile::gemm_tile<double>(d, 0, 0, gsm);
     }
-    if (!group_barrier(p.counter, (unsigned)G, epoch, p.st, p.limit_ns)) return;
+    // CTA 0's phase C reads only the block-row tile it has just written itself (c = j + 1), so it counts itself in
+    // and starts the diagonal block at once; the others wait for every block-row tile.
+    if (cta == 0 && G > 1) {
+      group_arrive(p.counter, epoch);
+    } else if (!group_barrier(p.counter, (unsigned)G, epoch, p.st, p.limit_ns)) {
+      return;
+    }
     // C: trailing update of the upper tiles (r, c), j < r <= c; CTA 0 takes (j+1, j+1) and then the next diagonal.
     const int m = nt - j - 1;
     if (cta == 0) {
