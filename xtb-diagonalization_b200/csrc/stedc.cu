@@ -202,7 +202,6 @@ __global__ void __launch_bounds__(1024) dc_deflate_kernel(DcBufs B, int nmerge) 
 
   // Small-z deflation, then the compacted list of candidates for pair deflation.
   int* ndl = B.ndl + s;
-  int* cand = B.cand + s;
   int m = 0;
   for (int base = 0; base < n; base += blockDim.x) {
     const int p = base + threadIdx.x;
@@ -217,27 +216,42 @@ __global__ void __launch_bounds__(1024) dc_deflate_kernel(DcBufs B, int nmerge) 
     m += tot;
     __syncthreads();
   }
-  for (int i = threadIdx.x; i < m - 1; i += blockDim.x) {
-    const int a = ndl[i], b = ndl[i + 1];
-    const double za = sz[a], zb = sz[b];
-    const double t = hypot(za, zb);
-    const double c = zb / t, sn = -za / t;
-    cand[i] = fabs((sd[b] - sd[a]) * c * sn) <= tol;
-  }
-  __syncthreads();
-
-  // Sequential chain of close-pair deflations (rare; the test of pair i uses the survivor of pair i-1).
-  if (threadIdx.x == 0) {
-    int nrot = 0;
-    bool modified = false;
-    for (int i = 0; i < m - 1; ++i) {
-      if (!cand[i] && !modified) continue;
+  // The pairs that pass the close-pair test before any rotation, compacted in pair order (the list borrows this
+  // merge's range of slotOf, which is written only further down).
+  int* clist = B.slotOf + s;
+  int nc = 0;
+  for (int base = 0; base < m - 1; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    int flag = 0;
+    if (i < m - 1) {
       const int a = ndl[i], b = ndl[i + 1];
       const double za = sz[a], zb = sz[b];
       const double t = hypot(za, zb);
       const double c = zb / t, sn = -za / t;
-      const double da = sd[a], db = sd[b];
-      if (fabs((db - da) * c * sn) <= tol) {
+      flag = fabs((sd[b] - sd[a]) * c * sn) <= tol;
+    }
+    int tot;
+    const int pre = block_exscan(flag, s_scan, &tot);
+    if (flag) clist[nc + pre] = i;
+    nc += tot;
+    __syncthreads();
+  }
+
+  // Sequential chain of close-pair deflations (rare; the test of pair i uses the survivor of pair i-1).  Thread 0
+  // visits only the candidates: from each one not yet examined it tests pairs i, i+1, ... until one does not
+  // deflate, which is the order and the set of tests of a scan over every pair.
+  if (threadIdx.x == 0) {
+    int nrot = 0, next = 0;
+    for (int q = 0; q < nc; ++q) {
+      int i = clist[q];
+      if (i < next) continue;
+      for (; i < m - 1; ++i) {
+        const int a = ndl[i], b = ndl[i + 1];
+        const double za = sz[a], zb = sz[b];
+        const double t = hypot(za, zb);
+        const double c = zb / t, sn = -za / t;
+        const double da = sd[a], db = sd[b];
+        if (!(fabs((db - da) * c * sn) <= tol)) break;
         sz[b] = t;
         sz[a] = 0.0;
         sd[a] = da * c * c + db * sn * sn;
@@ -249,10 +263,8 @@ __global__ void __launch_bounds__(1024) dc_deflate_kernel(DcBufs B, int nmerge) 
         B.rotc[s + nrot] = c;
         B.rots[s + nrot] = sn;
         ++nrot;
-        modified = true;
-      } else {
-        modified = false;
       }
+      next = i + 1;
     }
     s_cnt[0] = nrot;
   }
