@@ -568,7 +568,8 @@ __global__ void dc_order_kernel(DcBufs B, double* dnext) {
   const int s = md.s, n = md.n1 + md.n2, K = inf.K, nd = n - K;
   const double* lam = B.lam + s;
   const double* dv = B.dval + s;
-  for (int j = threadIdx.x; j < K; j += blockDim.x) {
+  const int first = blockIdx.y * blockDim.x + threadIdx.x, stride = gridDim.y * blockDim.x;
+  for (int j = first; j < K; j += stride) {
     const double x = lam[j];
     int c = 0;
     for (int t = 0; t < nd; ++t) c += okey(dv[t]) < okey(x);
@@ -576,7 +577,7 @@ __global__ void dc_order_kernel(DcBufs B, double* dnext) {
     B.outSrc[s + rank] = j;
     dnext[s + rank] = x;
   }
-  for (int t = threadIdx.x; t < nd; t += blockDim.x) {
+  for (int t = first; t < nd; t += stride) {
     const double x = dv[t];
     int lo = 0, hi = K;  // roots <= x
     while (lo < hi) { int m = (lo + hi) >> 1; if (okey(lam[m]) <= okey(x)) lo = m + 1; else hi = m; }
@@ -595,8 +596,8 @@ __global__ void dc_copy_kernel(DcBufs B) {
   const MergeInfo inf = B.info[mi];
   const int s = md.s, n = md.n1 + md.n2, K = inf.K;
   const size_t ld = B.ld;
-  const int c0 = blockIdx.y * 8;
-  for (int c = c0; c < min(c0 + 8, n); ++c) {
+  // One column per CTA (while the grid allows): enough CTAs in flight to cover the copy's memory latency.
+  for (int c = blockIdx.y; c < n; c += gridDim.y) {
     const int src = B.outSrc[s + c];
     const double* from = (src < K ? B.Qa : B.Qc) + (size_t)s + (size_t)(s + src) * ld;
     double* to = B.Qb + (size_t)s + (size_t)(s + c) * ld;
@@ -800,8 +801,8 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
     dc_zhat_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();
     dc_vectors_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();
     gemm_grouped_launch<double>(B.gdesc, 2 * nm, tiles[l], s);
-    dc_order_kernel<<<nm, maxn > 256 ? 256 : 128, 0, s>>>(B, dnext); note_launches();
-    dc_copy_kernel<<<dim3(nm, (maxn + 7) / 8), 128, 0, s>>>(B); note_launches();
+    dc_order_kernel<<<dim3(nm, (maxn + 255) / 256), 256, 0, s>>>(B, dnext); note_launches();
+    dc_copy_kernel<<<dim3(nm, std::min(maxn, 65535)), 256, 0, s>>>(B); note_launches();
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     // Next level reads (dd, Qa) = (dnext, Qb); the old Qa becomes the next output buffer.
