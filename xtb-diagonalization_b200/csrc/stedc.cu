@@ -373,7 +373,14 @@ __global__ void dc_gather_kernel(DcBufs B) {
   const double* qrow = B.Qa + (size_t)(s + r) + (size_t)s * ld;
   double* crow = B.Qc + (size_t)(s + r) + (size_t)s * ld;
   const int c1 = min(c0 + 32, n);
-  for (int col = c0; col < c1; ++col) crow[(size_t)col * ld] = qrow[(size_t)B.srcCol[s + col] * ld];
+  // All 32 loads before the first store: the stores could alias the loads for all the compiler knows, so a plain loop
+  // would wait one memory latency per column.
+  double v[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) v[k] = c0 + k < c1 ? qrow[(size_t)B.srcCol[s + c0 + k] * ld] : 0.0;
+#pragma unroll
+  for (int k = 0; k < 32; ++k)
+    if (c0 + k < c1) crow[(size_t)(c0 + k) * ld] = v[k];
 }
 
 // ------------------------------------------------------------------------------------------------ secular equation
