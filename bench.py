@@ -49,6 +49,10 @@ def parse():
     ap.add_argument("--cpu-budget-s", type=float, default=20.0, help="bound on the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-count", type=int, default=256, help="uneven batch size (0: skip the batch section)")
+    ap.add_argument("--cpu-batch-sample", type=int, default=64,
+                    help="problems of the CPU P x 1 batch protocol in the cpu_baseline leg (0: skip)")
+    ap.add_argument("--cpu-protocol", action="store_true",
+                    help="only the CPU baseline protocol of every configuration (no GPU): one JSON line")
     ap.add_argument("--batch-steps", type=int, default=3)
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision section")
     ap.add_argument("--no-autotune", action="store_true", help="use the default plan instead of autotuning it")
@@ -61,6 +65,62 @@ def parse():
 def rank_info():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
             int(os.environ.get("WORLD_SIZE", "1")))
+
+
+# ------------------------------------------------------------------------------------------------ inputs
+
+def build_generalized(n, seed):
+    """The generalized benchmark pair, built on the host with numpy's default_rng(seed) so that both bench arms (the
+    GPU path and the CPU LAPACK chain) solve the same bytes: S = I + G (G_ij = 0.35 exp(-|i-j|/12) u_ij, u ~ U[-1, 1]
+    drawn as a full n x n matrix of which the strict upper triangle is used, zero diagonal), shifted so that
+    lambda_min(S) >= 0.05; lam ~ U[-1.0, 0.5] Eh sorted, lam[n//2:] += 0.05 (the HOMO/LUMO gap); Q from the QR of a
+    standard normal n x n matrix (column signs fixed by R's diagonal); H = S^1/2 Q diag(lam) Q^T S^1/2 symmetrised.
+    Returns (H, S, lam) with H, S column-major float64 and lam the exact generalized spectrum (ascending).  Input
+    generation only, never timed."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    idx = np.arange(n)
+    dist = np.abs(idx[:, None] - idx[None, :])
+    u = rng.uniform(-1.0, 1.0, (n, n))
+    g = 0.35 * np.exp(-dist / 12.0) * np.triu(u, 1)
+    s = np.eye(n) + g + g.T
+    lmin = np.linalg.eigvalsh(s)[0]
+    if lmin < 0.05:
+        s += (0.05 - lmin) * np.eye(n)
+    lam = np.sort(rng.uniform(-1.0, 0.5, n))
+    lam[n // 2:] += 0.05
+    q, r = np.linalg.qr(rng.standard_normal((n, n)))
+    q = q * np.sign(np.diag(r))[None, :]
+    ws, vs = np.linalg.eigh(s)
+    shalf = (vs * np.sqrt(ws)[None, :]) @ vs.T
+    shalf = 0.5 * (shalf + shalf.T)
+    h = shalf @ ((q * lam[None, :]) @ q.T) @ shalf
+    h = 0.5 * (h + h.T)
+    return np.asfortranarray(h), np.asfortranarray(s), lam
+
+
+def bench_config(n, seed):
+    """The `config` object of both arms' lines (identical, so that the two arms are seen to run one workload)."""
+    return {"workload": f"generalized eigensolve H C = S C e, n={n}, seed={seed}, all eigenpairs, FP64 "
+                        "(potrf, sygst, sytrd, stedc, ormtr, trsm)",
+            "inputs": f"host numpy default_rng({seed}) construction (bench.build_generalized), the same bytes in both "
+                      "arms",
+            "l2": "GPU arm: flushed (256 MB write) before every timed step; CPU arm: n/a"}
+
+
+def host_cpu():
+    """nproc and the CPU model of this host."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return os.cpu_count(), model
 
 
 # ------------------------------------------------------------------------------------------------ clocks
@@ -141,13 +201,122 @@ def cpu_chain_time(h, s, budget_s: float, max_runs: int):
     return statistics.median(times), len(times), threads
 
 
+def cpu_one_thread_time(h, s, runs=3):
+    """The same chain with OpenBLAS on one thread (the reference's single-thread protocol): median ms of `runs` after
+    one untimed solve; the thread count is restored afterwards."""
+    from oracle import lapack
+
+    t_all = lapack.get_threads()
+    lapack.set_threads(1)
+    try:
+        lapack.sygvd_chain(h, s)
+        ts = []
+        for _ in range(runs):
+            t0 = time.perf_counter()
+            lapack.sygvd_chain(h, s)
+            ts.append((time.perf_counter() - t0) * 1e3)
+    finally:
+        lapack.set_threads(t_all)
+    return statistics.median(ts), runs
+
+
+def _cpu_batch_worker(jobs, barrier, out_q):
+    """One of P single-thread processes of the CPU batch protocol: builds its problems (untimed), waits for the other
+    processes, then solves them one after another with the LAPACK chain on one OpenBLAS thread."""
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    os.environ["OMP_NUM_THREADS"] = "1"
+    for p in (ROOT, PKG):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    from oracle import lapack
+
+    lapack.set_threads(1)
+    probs = [build_generalized(n, seed) for n, seed in jobs]
+    barrier.wait()
+    t0 = time.perf_counter()
+    for h, s, _ in probs:
+        lapack.sygvd_chain(h, s)
+    out_q.put((t0, time.perf_counter(), len(probs)))
+
+
+def cpu_batch_throughput(sample=64, procs=None):
+    """The reference's throughput protocol for the uneven batch (P processes x 1 thread, as its EigenBench sweeps,
+    Sources/EigenBench/main.swift:464-497): `sample` problems of the 256-size draw (every (256/sample)-th in draw
+    order; problem i built with seed 1000 + i), spread over P = nproc single-thread processes longest first (LPT by
+    n^3), timed from the moment every process has built its inputs until the last one finishes.  Returns jobs/s and
+    the sample's description.  Processes are started with `spawn` (never forked from a process that uses the GPU)."""
+    import multiprocessing as mp
+
+    sizes = batch_sizes(256, seed=3)
+    step = max(1, 256 // sample)
+    pick = list(range(0, 256, step))[:sample]
+    procs = procs or (os.cpu_count() or 1)
+    procs = max(1, min(procs, len(pick)))
+    load = [0.0] * procs
+    jobs = [[] for _ in range(procs)]
+    for i in sorted(pick, key=lambda i: -sizes[i] ** 3):
+        w = min(range(procs), key=lambda k: load[k])
+        jobs[w].append((sizes[i], 1000 + i))
+        load[w] += sizes[i] ** 3
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs)
+    out_q = ctx.Queue()
+    ps = [ctx.Process(target=_cpu_batch_worker, args=(jobs[k], barrier, out_q)) for k in range(procs)]
+    for p in ps:
+        p.start()
+    res = [out_q.get(timeout=1800) for _ in ps]
+    for p in ps:
+        p.join(timeout=60)
+    wall = max(r[1] for r in res) - min(r[0] for r in res)
+    return {"jobs_per_s": round(len(pick) / wall, 3), "processes": procs, "threads_per_process": 1,
+            "problems": len(pick), "wall_s": round(wall, 2),
+            "sample": f"{len(pick)} of the 256 uneven problems (every {step}th in draw order, sizes "
+                      f"{min(sizes[i] for i in pick)}-{max(sizes[i] for i in pick)}), built with numpy seeds 1000 + i"}
+
+
+def run_cpu_protocol(args):
+    """The CPU baseline protocol on this host (no GPU): the reference's LAPACK chain for configurations 1-3 on one
+    OpenBLAS thread and on all of them (median of 5 solves after one untimed solve, the reference's rule), and the
+    uneven batch as P = nproc processes x 1 thread over all 256 problems (jobs/s).  One JSON line."""
+    rank, _, _ = rank_info()
+    if rank != 0:
+        return
+    from oracle import inputs, lapack
+
+    nproc, model = host_cpu()
+    t_all = lapack.get_threads()
+    out = {"cpu_protocol": True, "host": {"nproc": nproc, "model": model, "openblas_threads_all": t_all},
+           "rule": "median of 5 after 1 untimed solve", "configs": {}}
+    cases = [("config1_standard_n412", "std", 412, 0), ("config2_generalized_n1204", "gen", 1204, 1),
+             ("config3_generalized_n1788", "gen", 1788, 2)]
+    for name, kind, n, seed in cases:
+        if kind == "std":
+            a, _ = inputs.standard(n, seed=seed)
+            run = lambda: lapack.syevd_chain(a)  # noqa: E731
+        else:
+            h, s, _ = build_generalized(n, seed)
+            run = lambda: lapack.sygvd_chain(h, s)  # noqa: E731
+        rec = {}
+        for label, threads in (("one_thread_ms", 1), ("all_cores_ms", t_all)):
+            lapack.set_threads(threads)
+            run()
+            ts = []
+            for _ in range(5):
+                t0 = time.perf_counter()
+                run()
+                ts.append((time.perf_counter() - t0) * 1e3)
+            rec[label] = round(statistics.median(ts), 3)
+        lapack.set_threads(t_all)
+        out["configs"][name] = rec
+    out["configs"]["config4_batch_256"] = cpu_batch_throughput(sample=256)
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args):
     rank, _, world = rank_info()
     if rank != 0:
         return
-    from oracle import inputs
-
-    h, s, _ = inputs.generalized(args.n, seed=args.seed)
+    h, s, _ = build_generalized(args.n, args.seed)
     from oracle import lapack
 
     warm = max(3, min(args.warmup, 5))  # untimed solves, as many as the GPU arm's (at least 3), at most 5 (~3 s)
@@ -158,12 +327,15 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world,
         "steps": runs, "warmup": warm, "ms_per_step": round(ms, 3), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generalized H, S)",
-        "config": {"workload": f"generalized eigensolve n={args.n} seed={args.seed}, all eigenpairs, FP64",
-                   "path": "LAPACK dpotrf,dsygst,dsytrd,dstedc,dormtr,dtrsm (OpenBLAS 0.3.30 from scipy)",
-                   "l2": "n/a (CPU)"},
-        "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": threads, "kind": "port",
-                         "sample": f"median of {runs} full solves (bounded to ~{int(budget)} s)"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generalized H, S; exact spectrum known)",
+        "config": bench_config(args.n, args.seed),
+        "details": {"path": "LAPACK dpotrf, dsygst, dsytrd, dstedc, dormtr, dtrsm (OpenBLAS 0.3.30 from scipy), "
+                            "the reference's own call chain", "host_cpu": host_cpu()[1]},
+        "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": host_cpu()[0], "threads": threads,
+                         "kind": "port",
+                         "sample": f"median of {runs} full solves on {threads} OpenBLAS threads (bounded to "
+                                   f"~{int(budget)} s)"},
         "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -496,23 +668,38 @@ def batch_sizes(count, seed=3, lo=124, hi=1788):
     return [int(x) for x in np.random.default_rng(seed).integers(lo, hi + 1, count)]
 
 
-def run_batch_section(args, dev, stream):
+def run_batch_section(args, dev, stream, rank=0, world=1):
     """The uneven batch: `count` generalized problems, sizes U[124, 1788] (seed 3), problem i built with seed
     1000 + i.  Device-resident batches through xtb_dsygvd_batched_device (restore of H, S inside each timed step),
     the same problems solved one at a time through xtb_dsygvd_device (per-size times), and one end-to-end batch
-    through xtb_dsygvd_batched from pinned host arrays."""
+    through xtb_dsygvd_batched from pinned host arrays.  With N ranks the batch is sharded: every rank builds and solves
+    only its own problems (xtb_batch_partition, longest first on the cost model of n; no exchange), and the batch
+    time is the maximum over ranks (one-at-a-time times are measured at N = 1 only)."""
     import ctypes
 
     import numpy as np
     import torch
 
+    import shard
     import xtbeig
 
     count = args.batch_count
-    sizes = batch_sizes(count, seed=3)
+    all_sizes = batch_sizes(count, seed=3)
+    mine = shard.my_problems(all_sizes, rank, world) if world > 1 else list(range(count))
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        import torch.distributed as dist
+
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    sizes = [all_sizes[i] for i in mine]
     t0 = time.perf_counter()
     H0, S0, LAM = [], [], []
-    for i, n in enumerate(sizes):
+    for i, n in zip(mine, sizes):
         h, s, lam = generalized_on_device(n, 1000 + i, dev)
         H0.append(h)
         S0.append(s)
@@ -524,8 +711,10 @@ def run_batch_section(args, dev, stream):
     W = [torch.empty(n, dtype=torch.float64, device=dev) for n in sizes]
     hp, sp, wp = [x.data_ptr() for x in H], [x.data_ptr() for x in S], [x.data_ptr() for x in W]
 
+    nloc = len(sizes)
+
     def batch_step():
-        for i in range(count):
+        for i in range(nloc):
             H[i].copy_(H0[i])
             S[i].copy_(S0[i])
         info, r = xtbeig.dsygvd_batched_device(sizes, hp, sizes, sp, sizes, wp, stream.cuda_stream)
@@ -547,8 +736,8 @@ def run_batch_section(args, dev, stream):
     torch.cuda.synchronize(dev)
     torch.cuda.nvtx.range_pop()
     launches = xtbeig.launch_count() - launches0
-    ms_batch = statistics.mean(a.elapsed_time(b) for a, b in ev)
-    eig_err = max(float((W[i] - LAM[i]).abs().max()) for i in range(count))
+    ms_batch = max_over_ranks(statistics.mean(a.elapsed_time(b) for a, b in ev))
+    eig_err = max_over_ranks(max(float((W[i] - LAM[i]).abs().max()) for i in range(nloc)))
 
     # The same batch in mixed precision (FP32 reduction chain + FP64 refinement).
     mixed = None
@@ -565,8 +754,8 @@ def run_batch_section(args, dev, stream):
                 batch_step()
                 evm[k][1].record(stream)
             torch.cuda.synchronize(dev)
-            ms_m = statistics.mean(a.elapsed_time(b) for a, b in evm)
-            err_m = max(float((W[i] - LAM[i]).abs().max()) for i in range(count))
+            ms_m = max_over_ranks(statistics.mean(a.elapsed_time(b) for a, b in evm))
+            err_m = max_over_ranks(max(float((W[i] - LAM[i]).abs().max()) for i in range(nloc)))
         finally:
             xtbeig.set_option("precision", prec0)
         mixed = {"solves_per_s": round(count / (ms_m * 1e-3), 2), "ms_per_batch": round(ms_m, 2), "steps": steps,
@@ -575,7 +764,7 @@ def run_batch_section(args, dev, stream):
 
     # One at a time: each problem alone on the caller's stream (eager, captured, then the timed replay).
     per = []
-    for i, n in enumerate(sizes):
+    for i, n in enumerate(sizes if world == 1 else []):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         for rep in range(3):
             H[i].copy_(H0[i])
@@ -588,7 +777,7 @@ def run_batch_section(args, dev, stream):
         e1.record(stream)
         torch.cuda.synchronize(dev)
         per.append(e0.elapsed_time(e1))
-    one_ms = sum(per)
+    one_ms = sum(per) if per else None
     bins = {}
     for lo, hi in ((124, 500), (500, 900), (900, 1300), (1300, 1789)):
         sel = [t for n, t in zip(sizes, per) if lo <= n < hi]
@@ -601,29 +790,33 @@ def run_batch_section(args, dev, stream):
     sh = [torch.empty((n, n), dtype=torch.float64, pin_memory=True) for n in sizes]
     wh = [torch.empty(n, dtype=torch.float64, pin_memory=True) for n in sizes]
     ns = np.array(sizes, np.int32)
-    ap = (ctypes.c_void_p * count)(*[x.data_ptr() for x in hh])
-    bp = (ctypes.c_void_p * count)(*[x.data_ptr() for x in sh])
-    wq = (ctypes.c_void_p * count)(*[x.data_ptr() for x in wh])
-    infos = np.zeros(count, np.int32)
+    ap = (ctypes.c_void_p * nloc)(*[x.data_ptr() for x in hh])
+    bp = (ctypes.c_void_p * nloc)(*[x.data_ptr() for x in sh])
+    wq = (ctypes.c_void_p * nloc)(*[x.data_ptr() for x in wh])
+    infos = np.zeros(nloc, np.int32)
     e2e = []
     for rep in range(2):
-        for i in range(count):
+        for i in range(nloc):
             hh[i].copy_(H0[i])
             sh[i].copy_(S0[i])
         t1 = time.perf_counter()
-        r = L.xtb_dsygvd_batched(count, xtbeig._p(ns), ap, xtbeig._p(ns), bp, xtbeig._p(ns), wq, xtbeig._p(infos))
-        dt = time.perf_counter() - t1
+        r = L.xtb_dsygvd_batched(nloc, xtbeig._p(ns), ap, xtbeig._p(ns), bp, xtbeig._p(ns), wq, xtbeig._p(infos))
+        dt = max_over_ranks(time.perf_counter() - t1)
         if r != 0:
             raise RuntimeError(f"xtb_dsygvd_batched returned {r}: {xtbeig.last_error()}")
         if rep == 1:
             e2e.append(dt)
-    elems = sum(n * n for n in sizes)
+    elems = sum(all_sizes[i] ** 2 for i in range(count))
     return {
         "count": count, "sizes": "uniform integers in [124, 1788], seed 3; problem i built with seed 1000 + i",
-        "workers": workers, "batch_grid": xtbeig.get_option("batch_grid"), "solves_per_s": round(count / (ms_batch * 1e-3), 2), "ms_per_batch": round(ms_batch, 2),
+        "sharding": (f"{world} ranks, each solving its own problems (xtb_batch_partition); times are the maximum over "
+                     "ranks" if world > 1 else "one GPU"),
+        "workers": workers, "batch_grid": xtbeig.get_option("batch_grid"),
+        "solves_per_s": round(count / (ms_batch * 1e-3), 2), "ms_per_batch": round(ms_batch, 2),
         "steps": steps, "warmup": 3, "gpu_launches_per_batch": int(launches // steps),
-        "one_at_a_time_solves_per_s": round(count / (one_ms * 1e-3), 2), "one_at_a_time_ms": round(one_ms, 2),
-        "speedup_vs_one_at_a_time": round(one_ms / ms_batch, 3), "per_size_ms_alone": bins,
+        "one_at_a_time_solves_per_s": round(count / (one_ms * 1e-3), 2) if one_ms else None,
+        "one_at_a_time_ms": round(one_ms, 2) if one_ms else None,
+        "speedup_vs_one_at_a_time": round(one_ms / ms_batch, 3) if one_ms else None, "per_size_ms_alone": bins,
         "eigenvalue_error_vs_exact_max": eig_err,
         "mixed": mixed,
         "e2e": {"solves_per_s": round(count / e2e[0], 2), "ms_per_batch": round(e2e[0] * 1e3, 2),
@@ -662,7 +855,11 @@ def run_ours(args):
         S0 = torch.from_numpy(np.ascontiguousarray(dump["s"])).to(dev)
         lam_t = None  # no exact spectrum: errors are reported against the FP64 GPU solve
     else:
-        H0, S0, lam_t = generalized_on_device(n, args.seed, dev)  # symmetric: row-major == column-major
+        # The same host-built bytes as the CPU arm (symmetric: row-major == column-major on the device).
+        h_np, s_np, lam_np = build_generalized(n, args.seed)
+        H0 = torch.from_numpy(np.ascontiguousarray(h_np)).to(dev)
+        S0 = torch.from_numpy(np.ascontiguousarray(s_np)).to(dev)
+        lam_t = torch.from_numpy(lam_np).to(dev)
     h_np, s_np = H0.cpu().numpy(), S0.cpu().numpy()
     H = torch.empty_like(H0)
     S = torch.empty_like(S0)
@@ -787,7 +984,7 @@ def run_ours(args):
             two_stage["mixed"] = run_variant_section(args, dev, stream, H0, S0, lam_t, flush,
                                                      {"autotune": 0, "reduction": 2, "band_width": 32,
                                                       "precision": 32})
-    batch = run_batch_section(args, dev, stream) if args.batch_count > 0 else None
+    batch = run_batch_section(args, dev, stream, rank, world) if args.batch_count > 0 else None
     adjoint = run_adjoint_section(args, dev) if args.adjoint_count > 0 else None
 
     if rank == 0:
@@ -798,19 +995,29 @@ def run_ours(args):
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             ms_cpu, runs, threads = cpu_chain_time(h_np, s_np, args.cpu_budget_s, 50)
-            cpu = {"value": round(ms_cpu, 3), "unit": "ms", "cores": threads, "kind": "port",
-                   "sample": f"median of {runs} full n={n} solves of the LAPACK chain (OpenBLAS), <= "
-                             f"{args.cpu_budget_s:.0f} s"}
+            ms_one, runs_one = cpu_one_thread_time(h_np, s_np)
+            nproc, model = host_cpu()
+            cpu = {"value": round(ms_cpu, 3), "unit": "ms", "cores": nproc, "threads": threads, "kind": "port",
+                   "sample": f"median of {runs} full n={n} solves of the LAPACK chain (OpenBLAS) on {threads} "
+                             f"threads, <= {args.cpu_budget_s:.0f} s",
+                   "one_thread": {"ms": round(ms_one, 3), "runs": runs_one,
+                                  "sample": f"median of {runs_one} full n={n} solves on 1 OpenBLAS thread"},
+                   "host_cpu": model}
+            if args.batch_count > 0 and args.cpu_batch_sample > 0:
+                cpu["batch_p_x_1"] = cpu_batch_throughput(args.cpu_batch_sample)
         total_stage = sum(v for _, v in stages) or 1.0
         line = {
             "metric": METRIC, "value": round(ms_step_max / world, 4), "unit": "ms", "n_gpus": world, "steps": K,
             "warmup": max(3, args.warmup), "ms_per_step": round(ms_step_max, 4), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generalized H, S; exact spectrum known)",
-            "config": {"workload": (f"generalized eigensolve of {os.path.basename(args.hs_bin)} n={n}" if args.hs_bin else
-                                    f"generalized eigensolve n={n} seed={args.seed}") + ", all eigenpairs, FP64 path",
-                       "eigenvalue_reference": eig_reference,
+            "config": ({"workload": f"generalized eigensolve of {os.path.basename(args.hs_bin)} n={n}, all "
+                                    "eigenpairs, FP64", "l2": "flushed (256 MB write) before every timed step"}
+                       if args.hs_bin else bench_config(n, args.seed)),
+            "details": {"eigenvalue_reference": eig_reference,
                        "path": "potrf, trtri, X^T H X, resident sytrd, D&C stedc, WY ormtr, X C' (all CUDA)",
+                       "multi_gpu": ("one GPU" if world == 1 else f"{world} independent replicas of the solve (a single "
+                                     "solve does not shard); value = max-over-ranks ms per step / N"),
                        "fp64_gemm_engine": ("int8 Ozaki splitting on tcgen05 for GEMMs >= 512^3 (exact int32 slice "
                                             "products, one FP64 rounding; FP64 accuracy), DMMA below"
                                             if (plans["fp64"]["dgemm"] if plans else
@@ -846,7 +1053,9 @@ def run_ours(args):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.cpu_protocol:
+        run_cpu_protocol(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -14,7 +14,8 @@
  *
  * Errors.  Entry points with an `info` argument report LAPACK-style info: 0 success, < 0 illegal argument,
  * > 0 numerical failure (stedc: an eigenvalue failed to converge; sygvd: info = n + i if the leading minor of order i
- * of B is not positive definite).  A CUDA failure (or a device wait that ran out of time) gives info = -1000 - code.
+ * of B is not positive definite).  A CUDA failure gives info = -1000 - cudaError; a device-side failure without a
+ * LAPACK meaning gives -2000 - its status code (a device wait that ran past "wait_limit_ms": -2001).
  * The sytrd/ormtr entries have no error channel (as in LAPACK); after any call xtb_gpu_last_status() returns 0 or the
  * failure code and xtb_gpu_last_error() a message.  Calls never abort the process.
  *
@@ -80,8 +81,9 @@ int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, 
  * and may synchronise the device).  The call allocates nothing: its scratch is a static device array of about
  * 57 KB that the library holds on every GPU it is loaded on.  Limits: 1 <= n <= XTB_NOALLOC_MAX_N (larger n
  * returns -1), lda >= n (else -3), and the device must hold the resident rows in shared memory (else -4; B200 does
- * for every n up to the maximum).  The first call on a device looks up the array's device address, so make it
- * before any stream capture.  Calls share the array: never let two calls overlap on the GPU.  Work is queued on
+ * for every n up to the maximum).  Every call looks up the array's device address; the first lookup on a device may
+ * load the library's device code there, so make the first call before any stream capture.  Calls share the array:
+ * never let two calls overlap on the GPU.  Its device waits use the "wait_limit_ms" option.  Work is queued on
  * `stream` (NULL: the legacy default stream) and the call synchronises it before returning 0, -1000 - cudaError,
  * or -2000 - device status code (e.g. a device wait that ran past its time limit). */
 #define XTB_NOALLOC_MAX_N 1792
@@ -155,6 +157,13 @@ int xtb_dsygvd_batched(int count, const int* n, double* const* a, const int* lda
  * replays each worker's captured graphs from its third call on (option "graphs"). */
 int xtb_dsygvd_batched_device(int count, const int* n, double* const* a, const int* lda, double* const* b,
                               const int* ldb, double* const* w, int* info, void* stream);
+/* Partition of a batch over `parts` GPUs or processes (no counterpart in the reference, which runs its throughput
+ * sweeps as independent processes, Sources/EigenBench/main.swift:464-497): part_of[i] in 0..parts-1 for problem i of
+ * size n[i], by the same longest-first assignment on the cost model of n that the batch calls use for their workers,
+ * so that every part gets about the same work.  The result depends only on (count, n, parts): every rank that calls
+ * it gets the same partition and solves its own problems with no exchange.  Host-only (no GPU needed).  Returns 0,
+ * -1 for count < 0, -2 for a NULL array or a negative n, -3 for parts < 1. */
+int xtb_batch_partition(int count, const int* n, int parts, int* part_of);
 
 /* Adjoint of the Fermi-smeared density matrix P = C diag(f) C^T, f_i = 2 / (1 + exp((e_i - mu)/kT)), where
  * H C = S C diag(e), C^T S C = I (H, S upper triangles, host arrays).  Given dL/dP = wbar (symmetric, n x n), returns
@@ -175,7 +184,8 @@ int xtb_dsygvd_density_adjoint_batched(int count, const int* n, const double* co
                                        const int* lddh, double* const* ds, const int* ldds, int* info);
 
 /* Options (process-wide): "sytrd_grid" (CTAs of the resident reduction, 0 = auto), "ormtr_nb" (reflectors per
- * compact-WY block, default 128), "wait_limit_ms" (device wait time limit, default 2000), "stage_timing" (1: record
+ * compact-WY block, default 128), "wait_limit_ms" (device wait time limit, 1 .. 600000, default 2000; a captured
+ * CUDA graph keeps the limit it was captured with), "stage_timing" (1: record
  * CUDA events at stage boundaries; read with xtb_gpu_stage_*), "graphs" (default 1: a device-pointer solve repeated
  * on the same buffers and non-NULL stream is captured into a CUDA graph on its second call and replayed after),
  * "batch_workers" (host threads, each with its own stream, that the batch calls spread problems over; default 8),
@@ -190,7 +200,10 @@ int xtb_dsygvd_density_adjoint_batched(int count, const int* n, const double* co
  * default; 2 = the same, and xtb_dgemm_device uses Ozaki at every size),
  * "batch_grid" (1, default: inside the batch calls, each problem's resident reduction takes the fewest CTAs that
  * hold its rows in shared memory, so that problems run side by side; the results are bit for bit those of single
- * solves; 0 = the single-solve grid).
+ * solves; 0 = the single-solve grid),
+ * "test_barrier_stall" (failure-detection test hook, default 0; 1: the resident reduction's grid barriers wait for one
+ * CTA more than the grid has, so every wait runs into "wait_limit_ms" and the call returns the barrier-timeout status
+ * -2001 (info) or 1 (xtb_gpu_last_status) instead of hanging; host-pointer calls only, never for production use).
  * Returns 0, -1 for an unknown name, or -2 for a value out of range. */
 int xtb_gpu_set_option(const char* name, long value);
 long xtb_gpu_get_option(const char* name);

@@ -56,3 +56,20 @@ def test_options_roundtrip_without_gpu():
     with pytest.raises(KeyError):
         xtbeig.set_option("no_such_option", 1)
     assert "sm_100a" in xtbeig.version()
+
+
+def test_wait_limit_and_test_hook_option_ranges_without_gpu():
+    """"wait_limit_ms" takes 1 .. 600000: a wait that gives up at once or never would defeat the limit."""
+    old = xtbeig.get_option("wait_limit_ms")
+    try:
+        for bad in (0, -1, -1000, 600001):
+            with pytest.raises(ValueError):
+                xtbeig.set_option("wait_limit_ms", bad)
+        assert xtbeig.get_option("wait_limit_ms") == old
+        xtbeig.set_option("wait_limit_ms", 1)
+        assert xtbeig.get_option("wait_limit_ms") == 1
+    finally:
+        xtbeig.set_option("wait_limit_ms", old)
+    assert xtbeig.get_option("test_barrier_stall") == 0
+    with pytest.raises(ValueError):
+        xtbeig.set_option("test_barrier_stall", 2)

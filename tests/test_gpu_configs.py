@@ -1,0 +1,116 @@
+"""Oracle parity on the benchmark configurations at their full sizes.
+
+The n = 1788 generalized pair (seed 2) is the configuration the benchmark times; the uneven batch draws 256 sizes
+uniform in [124, 1788] (seed 3, problem i built with seed 1000 + i).  Every result is compared with the oracle, the
+reference's LAPACK chain (dpotrf, dsygst, dsytrd, dstedc, dormtr, dtrsm) on the same input bytes, and with the exact
+spectrum the inputs are built with (the reference pins every variant to dsyevd on the same matrix,
+Sources/EigenBench/main.swift:505-531).
+
+Bars, FP64 path: eigenvalues within 1e-10 Eh of the oracle's and of the exact spectrum; backward error
+||HC - SCe||_F / (||H||_F n eps) <= 10; S-orthogonality max|C^T S C - I| <= 1e-12; aufbau density matrix (2 electrons
+in each of the n/2 lowest states, invariant to signs and rotations inside degenerate subspaces) within 1e-9 of the
+oracle's.  Mixed path (FP32 reduction chain + two FP64 refinement steps): the same, except S-orthogonality <= 1e-9.
+Two-stage mixed path: S-orthogonality <= 5e-9 (its 3xTF32 trailing updates start the refinement from vectors about
+ten times less accurate than the one-stage FP32 path's).
+"""
+import numpy as np
+import pytest
+
+from oracle import inputs, lapack, metrics
+
+pytestmark = pytest.mark.gpu
+
+N3, SEED3 = 1788, 2
+
+
+@pytest.fixture(scope="module")
+def config3():
+    h, s, lam = inputs.generalized(N3, seed=SEED3)
+    w_ref, c_ref = lapack.sygvd_chain(h, s)
+    return h, s, lam, w_ref, c_ref
+
+
+def _check(h, s, lam, w_ref, c_ref, w, c, orth_bar):
+    n = h.shape[0]
+    assert np.max(np.abs(w - w_ref)) <= 1e-10
+    assert np.max(np.abs(w - lam)) <= 1e-10
+    assert metrics.backward_error(h, s, w, c) <= 10
+    assert metrics.s_orthogonality(s, c) <= orth_bar
+    assert metrics.density_error(c, c_ref, metrics.aufbau(n, n // 2)) <= 1e-9
+
+
+@pytest.fixture
+def options(xe):
+    names = ("precision", "reduction", "band_width", "refine_iters", "autotune")
+    old = {k: xe.get_option(k) for k in names}
+    xe.set_option("autotune", 0)
+    yield xe
+    for k, v in old.items():
+        xe.set_option(k, v)
+
+
+def test_config3_fp64_n1788(options, config3):
+    h, s, lam, w_ref, c_ref = config3
+    w, c, u, info = options.dsygvd(h, s)
+    assert info == 0
+    _check(h, s, lam, w_ref, c_ref, w, c, 1e-12)
+    u_ref, _ = lapack.potrf_upper(s)
+    assert np.max(np.abs(np.triu(u) - u_ref)) < 1e-12
+
+
+def test_config3_mixed_n1788(options, config3):
+    options.set_option("precision", 32)
+    options.set_option("refine_iters", 2)
+    h, s, lam, w_ref, c_ref = config3
+    w, c, u, info = options.dsygvd(h, s)
+    assert info == 0
+    _check(h, s, lam, w_ref, c_ref, w, c, 1e-9)
+
+
+@pytest.mark.parametrize("b", [16, 32, 64])
+def test_config3_two_stage_fp64_n1788(options, config3, b):
+    options.set_option("reduction", 2)
+    options.set_option("band_width", b)
+    h, s, lam, w_ref, c_ref = config3
+    w, c, u, info = options.dsygvd(h, s)
+    assert info == 0
+    _check(h, s, lam, w_ref, c_ref, w, c, 1e-12)
+
+
+@pytest.mark.parametrize("b", [32, 64])
+def test_config3_two_stage_mixed_n1788(options, config3, b):
+    options.set_option("reduction", 2)
+    options.set_option("band_width", b)
+    options.set_option("precision", 32)
+    options.set_option("refine_iters", 2)
+    h, s, lam, w_ref, c_ref = config3
+    w, c, u, info = options.dsygvd(h, s)
+    assert info == 0
+    _check(h, s, lam, w_ref, c_ref, w, c, 5e-9)
+
+
+@pytest.fixture(scope="module")
+def config4_subset():
+    """The 16 smallest and the 16 largest problems of the 256-size draw, in draw order."""
+    sizes = inputs.batch_sizes(256, seed=3)
+    order = sorted(range(len(sizes)), key=lambda i: (sizes[i], i))
+    pick = sorted(order[:16] + order[-16:])
+    probs = []
+    for i in pick:
+        h, s, lam = inputs.generalized(sizes[i], seed=1000 + i)
+        w_ref, c_ref = lapack.sygvd_chain(h, s)
+        probs.append((h, s, lam, w_ref, c_ref))
+    return probs
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_config4_batch_subset_smallest_and_largest(options, config4_subset, precision):
+    options.set_option("precision", precision)
+    options.set_option("refine_iters", 2)
+    probs = config4_subset
+    assert max(p[0].shape[0] for p in probs) >= 1700 and min(p[0].shape[0] for p in probs) <= 130
+    w, c, u, info, ret = options.dsygvd_batched([p[0] for p in probs], [p[1] for p in probs])
+    assert ret == 0 and np.all(info == 0)
+    bar = 1e-12 if precision == 64 else 1e-9
+    for (h, s, lam, w_ref, c_ref), wi, ci in zip(probs, w, c):
+        _check(h, s, lam, w_ref, c_ref, wi, ci, bar)

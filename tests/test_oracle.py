@@ -158,3 +158,16 @@ def test_refine_oracle_cluster():
     assert np.max(np.abs(w - lam)) < 1e-12
     assert metrics.s_orthogonality(s, c) < 1e-10
     assert metrics.backward_error(h, s, w, c) < 10
+
+
+def test_bench_inputs_are_the_oracle_inputs():
+    """bench.py builds the timed pair itself (both bench arms solve those bytes); they must equal the oracle's."""
+    import bench
+
+    for n, seed in ((1, 0), (7, 3), (120, 2)):
+        h, s, lam = inputs.generalized(n, seed=seed)
+        hb, sb, lb = bench.build_generalized(n, seed)
+        np.testing.assert_array_equal(hb, h)
+        np.testing.assert_array_equal(sb, s)
+        np.testing.assert_array_equal(lb, lam)
+    assert bench.bench_config(1788, 2) == bench.bench_config(1788, 2)

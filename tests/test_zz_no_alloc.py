@@ -25,7 +25,7 @@ def _bind(xe):
     return fn
 
 
-def _run_noalloc(fn, a):
+def _run_noalloc(fn, a, stream=None):
     import torch
 
     n = a.shape[0]
@@ -36,9 +36,23 @@ def _run_noalloc(fn, a):
     e = torch.zeros(max(n - 1, 1), dtype=torch.float64, device=dev)
     tau = torch.zeros(max(n - 1, 1), dtype=torch.float64, device=dev)
     torch.cuda.synchronize(dev)
-    info = fn(n, ad.data_ptr(), n, d.data_ptr(), e.data_ptr(), tau.data_ptr(), None)
+    info = fn(n, ad.data_ptr(), n, d.data_ptr(), e.data_ptr(), tau.data_ptr(),
+              stream.cuda_stream if stream is not None else None)
     torch.cuda.synchronize(dev)
     return info, ad.cpu().numpy().T, d.cpu().numpy(), e.cpu().numpy()[: n - 1], tau.cpu().numpy()[: n - 1]
+
+
+def _check(a, out, ref):
+    n = a.shape[0]
+    info, ar, d, e, tau = out
+    ar_ref, d_ref, e_ref, tau_ref = ref
+    scale = np.abs(a).max() * n
+    assert info == 0, info
+    np.testing.assert_allclose(d, d_ref, rtol=0, atol=1e-11 * scale)
+    np.testing.assert_allclose(e, e_ref, rtol=0, atol=1e-11 * scale)
+    np.testing.assert_allclose(tau, tau_ref, rtol=0, atol=1e-11 * n)
+    np.testing.assert_allclose(np.triu(ar), np.triu(ar_ref), rtol=0, atol=1e-11 * n)
+    np.testing.assert_array_equal(np.tril(ar, -1), np.tril(a, -1))
 
 
 @pytest.mark.parametrize("n", [1, 2, 37, 300, 1788])
@@ -46,16 +60,33 @@ def test_noalloc_matches_existing_entry_point_twice(xe, n):
     fn = _bind(xe)
     xe.set_device(0)
     a = inputs.random_symmetric(n, seed=500 + n)
-    ar_ref, d_ref, e_ref, tau_ref = xe.sytrd_upper(a)
-    scale = np.abs(a).max() * n
+    ref = xe.sytrd_upper(a)
     for _ in range(2):
-        info, ar, d, e, tau = _run_noalloc(fn, a)
-        assert info == 0, info
-        np.testing.assert_allclose(d, d_ref, rtol=0, atol=1e-11 * scale)
-        np.testing.assert_allclose(e, e_ref, rtol=0, atol=1e-11 * scale)
-        np.testing.assert_allclose(tau, tau_ref, rtol=0, atol=1e-11 * n)
-        np.testing.assert_allclose(np.triu(ar), np.triu(ar_ref), rtol=0, atol=1e-11 * n)
-        np.testing.assert_array_equal(np.tril(ar, -1), np.tril(a, -1))
+        _check(a, _run_noalloc(fn, a), ref)
+
+
+def test_noalloc_on_a_side_stream_between_other_solves(xe):
+    """The static scratch keeps nothing that matters between calls: the entry point on a non-default stream, before
+    and after a device-pointer solve of the library's allocating path on the same device, gives the same result."""
+    import torch
+
+    fn = _bind(xe)
+    xe.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    n = 500
+    a = inputs.random_symmetric(n, seed=900)
+    ref = xe.sytrd_upper(a)
+    _check(a, _run_noalloc(fn, a, stream), ref)
+    h, s, lam = inputs.generalized(300, seed=901)
+    H = torch.from_numpy(np.ascontiguousarray(h)).to(dev)
+    S = torch.from_numpy(np.ascontiguousarray(s)).to(dev)
+    W = torch.empty(300, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    assert xe.dsygvd_device(300, H.data_ptr(), 300, S.data_ptr(), 300, W.data_ptr(), stream.cuda_stream) == 0
+    assert np.max(np.abs(W.cpu().numpy() - lam)) < 1e-10
+    _check(a, _run_noalloc(fn, a, stream), ref)
+    _check(a, _run_noalloc(fn, a), ref)
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit(xe):

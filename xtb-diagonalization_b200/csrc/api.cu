@@ -40,6 +40,7 @@ std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (
 std::atomic<long> g_autotune{0};      // 1: solves use the autotuned plan nearest their size (xtb_gpu_autotune)
 std::atomic<long> g_batch_grid{1};    // 1: batch workers size each resident reduction's grid to its matrix
 std::atomic<long> g_dgemm_engine{1};  // FP64 GEMMs: 0 DMMA, 1 Ozaki (int8 tcgen05) where eligible, 2 Ozaki always
+std::atomic<long> g_test_stall{0};    // failure-detection test hook: 1 makes the resident reduction's barriers unreachable
 
 // The tunable choices of one solve.  A solve resolves its plan once (options, or the autotuned table) and every stage
 // reads it from t_plan; the plan's signature is part of the graph-cache key, so a captured graph is never replayed
@@ -348,6 +349,7 @@ void stage_sytrd(Call& k, int n, const T* dfull, int ldf, T* dout, int lda, T* d
   p.ldr = pl.ldr;
   p.use_smem = pl.rows_in_smem ? 1 : 0;
   p.limit_ns = wait_limit_ns();
+  p.extra_members = g_test_stall.load() ? 1 : 0;
   if (!pl.rows_in_smem) {
     p.grows = k.template dev<T>("sytrd.rows", (size_t)pl.grid * pl.rows_per_cta * pl.ldr);
     if (!k.ok()) return;
@@ -836,6 +838,8 @@ void note_launches(int k) {
   g_launches.fetch_add(k, std::memory_order_relaxed);
   t_launches += k;
 }
+
+uint64_t option_wait_limit_ns() { return wait_limit_ns(); }
 
 }  // namespace xtbeig
 
@@ -1446,6 +1450,19 @@ int xtb_gpu_tuned_plan(int n, int precision, char* buf, int len) {
   return w;
 }
 
+int xtb_batch_partition(int count, const int* n, int parts, int* part_of) {
+  if (count < 0) return -1;
+  if (parts < 1) return -3;
+  if (count == 0) return 0;
+  if (!n || !part_of) return -2;
+  for (int i = 0; i < count; ++i)
+    if (n[i] < 0) return -2;
+  const std::vector<std::vector<int>> lists = lpt_assign(count, n, parts);
+  for (int p = 0; p < parts; ++p)
+    for (int i : lists[p]) part_of[i] = p;
+  return 0;
+}
+
 int xtb_dsygvd_batched(int count, const int* n, double* const* a, const int* lda, double* const* b, const int* ldb,
                        double* const* w, int* info) {
   const int bad = check_batch(count, n, a, lda, b, ldb, w);
@@ -1565,7 +1582,17 @@ int xtb_gpu_set_option(const char* name, long value) {
   if (!name) return -1;
   if (!std::strcmp(name, "sytrd_grid")) { g_sytrd_grid = value; return 0; }
   if (!std::strcmp(name, "ormtr_nb")) { g_ormtr_nb = value; return 0; }
-  if (!std::strcmp(name, "wait_limit_ms")) { g_wait_ms = value; return 0; }
+  if (!std::strcmp(name, "wait_limit_ms")) {
+    // 1 ms .. 10 min: a wait that gives up at once, or one that never gives up, would defeat the limit.
+    if (value < 1 || value > 600000) return -2;
+    g_wait_ms = value;
+    return 0;
+  }
+  if (!std::strcmp(name, "test_barrier_stall")) {
+    if (value != 0 && value != 1) return -2;
+    g_test_stall = value;
+    return 0;
+  }
   if (!std::strcmp(name, "stage_timing")) { g_stage_timing = value; return 0; }
   if (!std::strcmp(name, "graphs")) { g_graphs = value; return 0; }
   if (!std::strcmp(name, "batch_workers")) { g_batch_workers = value; return 0; }
@@ -1628,6 +1655,7 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "autotune")) return g_autotune;
   if (!std::strcmp(name, "dgemm_engine")) return g_dgemm_engine;
   if (!std::strcmp(name, "batch_grid")) return g_batch_grid;
+  if (!std::strcmp(name, "test_barrier_stall")) return g_test_stall;
   return -1;
 }
 

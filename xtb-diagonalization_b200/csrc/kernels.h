@@ -11,6 +11,8 @@ namespace xtbeig {
 
 // Count of kernel launches issued by the library (all threads); read through xtb_gpu_launch_count().
 void note_launches(int k = 1);
+// The device wait time limit of the option "wait_limit_ms", in nanoseconds.
+uint64_t option_wait_limit_ns();
 
 // ---------------------------------------------------------------------------------------------------- sytrd
 template <typename T>
@@ -31,6 +33,10 @@ struct SytrdParams {
   int ldr;
   int use_smem;
   uint64_t limit_ns;
+  // Members the grid barriers wait for beyond the grid itself: 0 in every solve.  The library's failure-detection
+  // test hook (option "test_barrier_stall") sets 1, so that no barrier can complete and every wait runs into its
+  // time limit and returns an error status instead of hanging.
+  int extra_members;
 };
 
 struct SytrdPlan {

@@ -6,14 +6,15 @@
 // status word and the two double-buffered exchange vectors) lives in the file-scope array below, which every GPU that
 // loads the library holds until the process exits.
 //
-// Host code may not use the array's name as a device address (on the host it names a stand-in object): the device
-// address is looked up once per device with cudaGetSymbolAddress, on the first call made with that device current,
-// so that first call should come before any stream capture.  Every call shares the array and it keeps the last
-// call's contents, so each call clears the status word and the barrier counter before its launch; calls whose work
-// overlaps on the GPU (two streams, or two threads, at the same time) race on the array and must not be issued.
+// Host code may not use the array's name as a device address (on the host it names a stand-in object): every call
+// looks the device address up with cudaGetSymbolAddress on the current device.  The lookup is a host-side query,
+// except that the first one on a device may load the library's device code there, so that first call should come
+// before any stream capture.  Looking the address up per call (instead of caching it per device) keeps the entry
+// point valid after a cudaDeviceReset, which may give the array a new address.  Every call shares the array and it
+// keeps the last call's contents, so each call clears the status word and the barrier counter before its launch;
+// calls whose work overlaps on the GPU (two streams, or two threads, at the same time) race on the array and must
+// not be issued.  The barrier waits use the time limit of the option "wait_limit_ms".
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "../../include/xtb_eig.h"
 #include "kernels.h"
@@ -29,21 +30,12 @@ constexpr size_t kScratchBytes = kVectorOffset + 4 * (size_t)kMaxN * sizeof(doub
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-void* g_scratch_address[kMaxDevices];
-std::mutex g_setup_mutex;
-
-// Device address of g_noalloc_scratch on `dev` (current), looked up on the first call for that device.
-cudaError_t scratch_address(int dev, unsigned char** out) {
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_address[dev]) {
-    void* ptr = nullptr;
-    const cudaError_t err = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if (err != cudaSuccess) return err;
-    g_scratch_address[dev] = ptr;
-  }
-  *out = static_cast<unsigned char*>(g_scratch_address[dev]);
+// Device address of g_noalloc_scratch on the current device.
+cudaError_t scratch_address(unsigned char** out) {
+  void* ptr = nullptr;
+  const cudaError_t err = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  if (err != cudaSuccess) return err;
+  *out = static_cast<unsigned char*>(ptr);
   return cudaSuccess;
 }
 
@@ -62,7 +54,7 @@ extern "C" int xtb_dsytrd_upper_noalloc(int n, double* a, int lda, double* d, do
   if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (err == cudaSuccess) err = cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   unsigned char* base = nullptr;
-  if (err == cudaSuccess) err = scratch_address(dev, &base);
+  if (err == cudaSuccess) err = scratch_address(&base);
   if (err != cudaSuccess) return -1000 - (int)err;
   const SytrdPlan pl = sytrd_plan<double>(n, sms, (size_t)smem > 2048 ? (size_t)smem - 2048 : (size_t)smem, 0);
   if (!pl.rows_in_smem || pl.threads != 512 || pl.cpt > 4) return -4;
@@ -83,7 +75,7 @@ extern "C" int xtb_dsytrd_upper_noalloc(int n, double* a, int lda, double* d, do
   p.rows_per_cta = pl.rows_per_cta;
   p.ldr = pl.ldr;
   p.use_smem = 1;
-  p.limit_ns = 2000000000ull;
+  p.limit_ns = option_wait_limit_ns();
   // Status word and barrier counter must start at zero; the exchange vectors are written before they are read.
   err = cudaMemsetAsync(base, 0, kVectorOffset, s);
   if (err == cudaSuccess) err = sytrd_launch_upper_inplace(p, pl, s);

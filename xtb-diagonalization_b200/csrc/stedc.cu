@@ -566,7 +566,8 @@ __global__ void dc_vectors_kernel(DcBufs B) {
 
 // ------------------------------------------------------------------------------------------------ final order
 
-// One CTA per merge: rank of every root and deflated value in the merged ascending order.
+// grid (merges, column groups): rank of every root and deflated value in the merged ascending order; the CTAs of a
+// merge (blockIdx.y) split its roots and deflated values between them with a grid-stride loop.
 __global__ void dc_order_kernel(DcBufs B, double* dnext) {
   DC_RETURN_IF_FAILED(B)
   const int mi = blockIdx.x;
@@ -595,7 +596,8 @@ __global__ void dc_order_kernel(DcBufs B, double* dnext) {
   }
 }
 
-// grid (merges, column blocks of 8): copy each output column into the next level's eigenvector matrix.
+// grid (merges, columns): copy each output column into the next level's eigenvector matrix, one column per CTA with a
+// grid-stride loop over the merge's columns.
 __global__ void dc_copy_kernel(DcBufs B) {
   DC_RETURN_IF_FAILED(B)
   const int mi = blockIdx.x;

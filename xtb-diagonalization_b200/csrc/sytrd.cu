@@ -144,8 +144,9 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
   __syncthreads();
 
   unsigned epoch = 0;
+  const unsigned members = (unsigned)(G + p.extra_members);
   if constexpr (kUpperInPlace) {
-    if (!group_barrier(p.counter, (unsigned)G, epoch, p.st, p.limit_ns)) return;
+    if (!group_barrier(p.counter, members, epoch, p.st, p.limit_ns)) return;
   }
   for (int k = n - 1; k >= 1; --k) {
     const int t = n - 1 - k;                   // step index
@@ -241,7 +242,7 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
         st_pair(xch + 2 * (size_t)r, y, colk[q]);
       }
     }
-    if (!group_barrier(p.counter, (unsigned)G, epoch, p.st, p.limit_ns)) return;
+    if (!group_barrier(p.counter, members, epoch, p.st, p.limit_ns)) return;
     T yj[CPT], colj[CPT];
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
