@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--cpu-budget-s", type=float, default=20.0, help="bound on the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-count", type=int, default=256, help="uneven batch size (0: skip the batch section)")
-    ap.add_argument("--cpu-batch-sample", type=int, default=64,
+    ap.add_argument("--cpu-batch-sample", type=int, default=256,
                     help="problems of the CPU P x 1 batch protocol in the cpu_baseline leg (0: skip)")
     ap.add_argument("--cpu-protocol", action="store_true",
                     help="only the CPU baseline protocol of every configuration (no GPU): one JSON line")
