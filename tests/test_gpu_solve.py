@@ -280,3 +280,30 @@ def test_device_api_repeated_calls_graph_replay(xe, graphs):
         np.testing.assert_array_equal(c, outs[0][1])
     np.testing.assert_allclose(outs[0][0], w_ref, rtol=0, atol=1e-12)
     assert metrics.density_error(outs[0][1], c_ref, metrics.aufbau(n, n // 2)) < 1e-9
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_backtransform_orders_agree(xe, precision):
+    """Option "backtransform": 1 (default) forms X Q beside the tridiagonal eigensolve and finishes with C = (X Q) Z;
+    0 applies ormtr to Z and then X.  Both orders meet the bars against the oracle on the same input, and their
+    eigenvalues agree to rounding."""
+    n = 700
+    h, s, lam = inputs.generalized(n, seed=90)
+    w_ref, c_ref = lapack.sygvd_chain(h, s)
+    old = (xe.get_option("backtransform"), xe.get_option("precision"))
+    out = {}
+    try:
+        xe.set_option("precision", precision)
+        for order in (0, 1):
+            xe.set_option("backtransform", order)
+            w, c, u, info = xe.dsygvd(h, s)
+            assert info == 0
+            assert np.max(np.abs(w - lam)) < 1e-10 and np.max(np.abs(w - w_ref)) < 1e-10
+            assert metrics.backward_error(h, s, w, c) < 10
+            assert metrics.s_orthogonality(s, c) < (1e-12 if precision == 64 else 1e-9)
+            assert metrics.density_error(c, c_ref, metrics.aufbau(n, n // 2)) < 1e-9
+            out[order] = w
+    finally:
+        xe.set_option("backtransform", old[0])
+        xe.set_option("precision", old[1])
+    assert np.max(np.abs(out[0] - out[1])) < 1e-12

@@ -40,6 +40,7 @@ std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (
 std::atomic<long> g_autotune{0};      // 1: solves use the autotuned plan nearest their size (xtb_gpu_autotune)
 std::atomic<long> g_batch_grid{1};    // 1: batch workers size each resident reduction's grid to its matrix
 std::atomic<long> g_dgemm_engine{1};  // FP64 GEMMs: 0 DMMA, 1 Ozaki (int8 tcgen05) where eligible, 2 Ozaki always
+std::atomic<long> g_backtransform{1};  // 1: C = (X Q) Z with X Q formed beside the tridiagonal eigensolve (n >= 512)
 std::atomic<long> g_test_stall{0};    // failure-detection test hook: 1 makes the resident reduction's barriers unreachable
 
 // The tunable choices of one solve.  A solve resolves its plan once (options, or the autotuned table) and every stage
@@ -53,10 +54,11 @@ struct Plan {
   int mixed_gemm = 3;  // FP32 GEMM engine of the mixed path
   int dgemm = 0;       // FP64 GEMM engine of the large GEMMs: 0 DMMA, 1 or 2 int8 Ozaki
   int batch_grid = 0;  // 1: a batch worker's solve, its resident reduction sized to its matrix (sytrd_grid 0)
+  int xq = 1;          // generalized one-stage solves with n >= kXqMinN: C = (X Q) Z, X Q formed beside the D&C
   double ms = 0.0;     // measured time of the tuned plan
   long long sig() const {
     return (long long)reduction | (long long)band << 4 | (long long)sytrd_grid << 12 | (long long)ormtr_nb << 24 |
-           (long long)mixed_gemm << 36 | (long long)dgemm << 40 | (long long)batch_grid << 42;
+           (long long)mixed_gemm << 36 | (long long)dgemm << 40 | (long long)batch_grid << 42 | (long long)xq << 43;
   }
 };
 
@@ -74,6 +76,7 @@ Plan options_plan() {
   p.ormtr_nb = (int)g_ormtr_nb.load();
   p.mixed_gemm = (int)g_mixed_gemm.load();
   p.dgemm = (int)g_dgemm_engine.load();
+  p.xq = (int)g_backtransform.load();
   return p;
 }
 
@@ -386,6 +389,7 @@ struct Reduction {
   T* r = nullptr;    // one stage: LAPACK-layout reflectors
   T* tau = nullptr;
   bool prepared = false;  // one stage: ormtr's V, T, Y being built on the aux stream (joined before the apply)
+  bool xq = false;        // one stage: X Q formed on the aux stream as well (joined before C = (X Q) Z)
   int nb = 0;
   OrmtrWork<T> ow{};
   T* v1 = nullptr;   // two stages
@@ -413,8 +417,13 @@ bool ensure_aux_stream(Context* c) {
 // `back`: the caller will back-transform n columns, so the one-stage path starts ormtr's preparation (V, T, Y from the
 // reflectors) on the aux stream right after the reduction, overlapping the tridiagonal eigensolve; stage_backtransform
 // joins it.
+// `xq_x` (upper triangular, ld xq_ldx): the caller back-transforms to the generalized basis with C = X Q Z; the
+// one-stage path then also forms Q explicitly (ormtr applied to the identity, into xq_q) and M = X Q (into xq_m) on
+// the aux stream, so that after the tridiagonal eigensolve one GEMM C = M Z remains on the critical path instead of
+// ormtr's apply and the triangular product.
 template <typename T>
-Reduction<T> stage_reduce(Call& k, const char* pre, int n, T* f, T* d, T* e, const TcGemm& tc, bool back = true) {
+Reduction<T> stage_reduce(Call& k, const char* pre, int n, T* f, T* d, T* e, const TcGemm& tc, bool back = true,
+                          const T* xq_x = nullptr, int xq_ldx = 0, T* xq_q = nullptr, T* xq_m = nullptr) {
   Reduction<T> red;
   int b = 0;
   if (!k.ok()) return red;
@@ -438,6 +447,13 @@ Reduction<T> stage_reduce(Call& k, const char* pre, int n, T* f, T* d, T* e, con
       k.check(cudaStreamWaitEvent(k.c->aux, k.c->ev_fork, 0), "fork wait");
       if (k.ok())
         k.check(ormtr_prepare<T>(n, red.r, n, red.tau, red.nb, red.ow, k.c->arena, k.c->aux, tc), "ormtr prepare");
+      if (xq_x && k.ok()) {
+        set_identity<T>(n, xq_q, n, k.c->aux);
+        k.check(ormtr_apply<T>(n, n, xq_q, n, red.nb, red.ow, k.c->arena, k.c->aux, tc), "Q formation");
+        GemmDesc<T> p = gemm_problem<T>(n, n, n, T(1), xq_x, xq_ldx, 0, xq_q, n, 0, T(0), xq_m, n, kTriAUpper);
+        if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.c->aux), "X Q");
+        red.xq = true;
+      }
       // Joined in stage_backtransform; recorded even after a failure so that a capture can always be closed.
       const cudaError_t je = cudaEventRecord(k.c->ev_join, k.c->aux);
       if (k.ok()) k.check(je, "join record");
@@ -484,6 +500,25 @@ void stage_backtransform(Call& k, const char* pre, int n, int m, const Reduction
   k.mark("q2");
   if (k.ok()) k.check(q1_apply<T>(n, red.b, m, red.v1, red.t1, z, ldz, w, k.c->arena, tc, k.s), "Q1 back-transform");
   k.mark("q1");
+}
+
+// Generalized one-stage solves from this size up form X Q beside the tridiagonal eigensolve (below it the side work
+// does not hide behind the D&C and the classic order is as fast).
+constexpr int kXqMinN = 512;
+bool use_xq(Call& k, int n) {
+  int b = 0;
+  return t_plan.xq == 1 && n >= kXqMinN && !(t_plan.reduction == 2 && two_stage_plan<double>(k, n, &b));
+}
+
+// The C = (X Q) Z step after the tridiagonal eigensolve: waits for the aux stream's X Q, then one GEMM.
+template <typename T>
+void stage_xq_backtransform(Call& k, int n, const T* m, const T* z, T* c, const TcGemm& tc) {
+  if (!k.ok()) return;
+  k.check(cudaStreamWaitEvent(k.s, k.c->ev_join, 0), "join");
+  k.mark("xq_join");
+  GemmDesc<T> p = gemm_problem<T>(n, n, n, T(1), m, n, 0, z, n, 0, T(0), c, n);
+  if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "C = (X Q) Z");
+  k.mark("backtransform");
 }
 
 // The tcgen05 engine for the FP32 GEMMs of an n x n mixed solve (passes from the mixed_gemm option; 0 = CUDA cores).
@@ -564,9 +599,17 @@ void solve_factored_fp64(Call& k, int n, double* h, const double* x, int ldx, do
   if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "congruence 2");
   if (k.ok()) symmetrize_upper<double>(n, hp, n, h, n, k.s);
   k.mark("congruence");
-  const Reduction<double> red = stage_reduce<double>(k, "gv.", n, h, w, e, tc);
+  const bool xq = use_xq(k, n);
+  double* qx = xq ? k.template dev<double>("gv.Qx", (size_t)n * n) : nullptr;
+  double* mx = xq ? k.template dev<double>("gv.M", (size_t)n * n) : nullptr;
+  if (!k.ok()) return;
+  const Reduction<double> red = stage_reduce<double>(k, "gv.", n, h, w, e, tc, true, xq ? x : nullptr, ldx, qx, mx);
   stage_stedc(k, n, w, e, z, n);
   k.mark("stedc");
+  if (red.xq) {
+    stage_xq_backtransform<double>(k, n, mx, z, c, tc);
+    return;
+  }
   stage_backtransform<double>(k, "gv.", n, n, red, z, n, tc);
   // C = X Z (X upper).
   p = gemm_problem<double>(n, n, n, 1.0, x, ldx, 0, z, n, 0, 0.0, c, n, kTriAUpper);
@@ -603,7 +646,11 @@ void solve_factored_mixed(Call& k, int n, double* h, const double* u, int ldu, c
   if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "congruence 2 (fp32)");
   if (k.ok()) symmetrize_upper<float>(n, rf, n, hf, n, k.s);
   k.mark("congruence");
-  const Reduction<float> red = stage_reduce<float>(k, "mx.", n, hf, df, ef, tc);
+  const bool xq = use_xq(k, n);
+  float* qxf = xq ? k.template dev<float>("mx.Qx", 2 * nn) : nullptr;
+  float* mxf = xq ? qxf + nn : nullptr;
+  if (!k.ok()) return;
+  const Reduction<float> red = stage_reduce<float>(k, "mx.", n, hf, df, ef, tc, true, xq ? xf : nullptr, n, qxf, mxf);
   if (k.ok()) {
     convert_f32_to_f64(n, df, w, k.s);
     convert_f32_to_f64(n, ef, e, k.s);
@@ -611,11 +658,15 @@ void solve_factored_mixed(Call& k, int n, double* h, const double* u, int ldu, c
   stage_stedc(k, n, w, e, z, n);
   k.mark("stedc");
   if (k.ok()) convert_mat_f64_to_f32(n, n, z, n, zf, n, k.s);
-  stage_backtransform<float>(k, "mx.", n, n, red, zf, n, tc);
-  p = gemm_problem<float>(n, n, n, 1.f, xf, n, 0, zf, n, 0, 0.f, tf, n, kTriAUpper);
-  if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "back-transform (fp32)");
+  if (red.xq) {
+    stage_xq_backtransform<float>(k, n, mxf, zf, tf, tc);
+  } else {
+    stage_backtransform<float>(k, "mx.", n, n, red, zf, n, tc);
+    p = gemm_problem<float>(n, n, n, 1.f, xf, n, 0, zf, n, 0, 0.f, tf, n, kTriAUpper);
+    if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "back-transform (fp32)");
+    k.mark("trmm");
+  }
   if (k.ok()) convert_mat_f32_to_f64(n, n, tf, n, c, n, k.s);
-  k.mark("trmm");
   if (k.ok())
     k.check(refine_generalized(n, h, n, nullptr, 0, u, ldu, c, n, w, (int)g_refine_iters.load(), rw, k.c->arena,
                                k.s, &tc),
@@ -1593,6 +1644,11 @@ int xtb_gpu_set_option(const char* name, long value) {
     g_test_stall = value;
     return 0;
   }
+  if (!std::strcmp(name, "backtransform")) {
+    if (value != 0 && value != 1) return -2;
+    g_backtransform = value;
+    return 0;
+  }
   if (!std::strcmp(name, "stage_timing")) { g_stage_timing = value; return 0; }
   if (!std::strcmp(name, "graphs")) { g_graphs = value; return 0; }
   if (!std::strcmp(name, "batch_workers")) { g_batch_workers = value; return 0; }
@@ -1656,6 +1712,7 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "dgemm_engine")) return g_dgemm_engine;
   if (!std::strcmp(name, "batch_grid")) return g_batch_grid;
   if (!std::strcmp(name, "test_barrier_stall")) return g_test_stall;
+  if (!std::strcmp(name, "backtransform")) return g_backtransform;
   return -1;
 }
 
