@@ -191,7 +191,10 @@ int xtb_dsygvd_density_adjoint_batched(int count, const int* n, const double* co
  * "batch_workers" (host threads, each with its own stream, that the batch calls spread problems over; default 8),
  * "precision" (64, default: FP64 throughout; 32: the generalized solves run the reduction chain in FP32 - congruence,
  * resident sytrd, ormtr, back-transform; Cholesky and the tridiagonal eigensolve stay FP64 - then refine C and e in
- * FP64 as xtb_dsygvd_refine_device does), "refine_iters" (refinement steps of the mixed path, default 2),
+ * FP64 as xtb_dsygvd_refine_device does), "refine_iters" (refinement steps of the mixed path, default 2; 0 keeps the
+ * plain FP32 vectors, about 1e-6 accurate), "backtransform" (1, default: generalized one-stage solves with n >= 512
+ * form Q and X Q = U^-1 Q beside the tridiagonal eigensolve and finish with one GEMM C = (X Q) Z; 0: ormtr on Z, then
+ * X (Q Z)),
  * "mixed_gemm" (engine of the mixed path's FP32 GEMMs: 3 = 3xTF32 on the tcgen05 tensor cores, default; 1 = TF32;
  * 0 = FP32 on the CUDA cores), "reduction" (1 = one-stage resident sytrd, default; 2 = two-stage sy2sb + sb2st),
  * "band_width" (two-stage band width 16, 32 default, 64), "autotune" (1: use xtb_gpu_autotune's plans),
@@ -207,6 +210,23 @@ int xtb_dsygvd_density_adjoint_batched(int count, const int* n, const double* co
  * Returns 0, -1 for an unknown name, or -2 for a value out of range. */
 int xtb_gpu_set_option(const char* name, long value);
 long xtb_gpu_get_option(const char* name);
+
+/* SCC precision policy of the calling thread: the library-side form of xtb's FP32-early / FP64-to-convergence switch
+ * with its FP64 restart (xtb_setSCCPrecision, reference LOG.md:317-363).  xtb_gpu_scc_set_precision(fp32_rmsq,
+ * fp32_maxiter, fp32_refine) starts a run: fp32_rmsq > 0 turns the policy on (0: off, every solve follows the
+ * "precision" option), fp32_refine 1 refines the FP32 vectors in FP64 ("refine_iters" steps), 0 keeps plain FP32
+ * vectors (xtb's default FP32 mode).  Returns 0, or -1 / -2 / -3 for a negative or non-finite fp32_rmsq, fp32_maxiter
+ * < 1, or fp32_refine not 0 or 1.  xtb_gpu_scc_cycle(cycle, rmsq) is called at the start of every SCC cycle (cycle
+ * 1, 2, ...; rmsq = the last density update's RMS change, negative if unknown) and sets the precision of the
+ * thread's following solves, batch calls included: 32 while rmsq > fp32_rmsq (and in cycle 1), then 64 for the rest
+ * of the run once rmsq has dropped to fp32_rmsq or below.  It returns that precision, or 0 when the run used FP32
+ * and reached cycle fp32_maxiter + 1 without converging: the caller then reruns the SCC from its start and every
+ * solve of the rerun is FP64.  xtb_gpu_scc_report gives the cycles solved in FP32, whether the restart happened and
+ * the precision in effect; it returns 1 if the policy is on.  The policy and its overrides belong to the calling
+ * thread only. */
+int xtb_gpu_scc_set_precision(double fp32_rmsq, int fp32_maxiter, int fp32_refine);
+int xtb_gpu_scc_cycle(int cycle, double rmsq);
+int xtb_gpu_scc_report(int* fp32_cycles, int* restarted, int* precision);
 
 /* Device of the calling thread's later calls (the library keeps its own CUDA runtime state, so a caller that selects
  * devices through another runtime, e.g. a Python framework, states the device here).  Returns 0 or -1000 - code. */

@@ -143,3 +143,38 @@ def test_refine_device_invalid_arguments(xe):
     assert xe.dsygvd_refine_device(0, 0, 1, 0, 1, 0, 1, 0, 2) == 0
     with pytest.raises(ValueError):
         xe.set_option("precision", 16)
+
+
+def test_scc_policy_sets_the_precision_of_solves(xe):
+    """The SCC precision policy of the calling thread: a cycle above the rmsq threshold solves in plain FP32 (about
+    1e-6 accurate, xtb's FP32 mode) or FP32 + FP64 refinement (fp32_refine 1: the mixed path's bars); a cycle below
+    it solves in FP64, bit for bit as the FP64 path; after fp32_maxiter cycles the run restarts in FP64."""
+    n = 400
+    h, s, lam = inputs.generalized(n, seed=95)
+    w_ref, c_ref = lapack.sygvd_chain(h, s)
+    w64, c64, _, info = xe.dsygvd(h, s)
+    assert info == 0
+    try:
+        xe.scc_set_precision(1e-3, fp32_maxiter=30, fp32_refine=0)
+        assert xe.scc_cycle(1, -1.0) == 32
+        w, c, _, info = xe.dsygvd(h, s)
+        assert info == 0
+        err = np.max(np.abs(w - lam))
+        assert 1e-13 < err < 1e-4, err  # plain FP32 vectors: neither FP64-exact nor wrong
+        assert metrics.density_error(c, c_ref, metrics.aufbau(n, n // 2)) < 1e-3
+        assert xe.scc_cycle(2, 1e-4) == 64
+        w, c, _, info = xe.dsygvd(h, s)
+        assert info == 0
+        np.testing.assert_array_equal(w, w64)
+        np.testing.assert_array_equal(c, c64)
+        xe.scc_set_precision(1e-3, fp32_maxiter=1, fp32_refine=1)
+        assert xe.scc_cycle(1, -1.0) == 32
+        w, c, _, info = xe.dsygvd(h, s)
+        assert info == 0
+        _check(h, s, lam, w, c, w_ref, c_ref, n // 2)
+        assert xe.scc_cycle(2, 1e-2) == 0  # used FP32, not converged within 1 cycle: rerun in FP64
+        assert xe.scc_cycle(1, -1.0) == 64
+        w, c, _, info = xe.dsygvd(h, s)
+        np.testing.assert_array_equal(w, w64)
+    finally:
+        xe.scc_set_precision(0.0)

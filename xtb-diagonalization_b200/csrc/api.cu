@@ -34,6 +34,23 @@ std::atomic<long> g_graphs{1};
 std::atomic<long> g_batch_workers{8};
 std::atomic<long> g_precision{64};    // 64: FP64 throughout; 32: FP32 reduction chain + FP64 refinement
 std::atomic<long> g_refine_iters{2};
+// Per-thread overrides of "precision" and "refine_iters" set by the SCC precision policy (0 / -1: use the options).
+thread_local long t_prec_override = 0;
+thread_local long t_refine_override = -1;
+// The SCC precision policy of one thread (xtb_gpu_scc_set_precision / xtb_gpu_scc_cycle).
+struct SccPolicy {
+  bool on = false;
+  double rmsq = 0.0;
+  int maxiter = 160;
+  int refine = 0;
+  bool latched64 = false;
+  bool restarted = false;
+  int fp32_cycles = 0;
+  int cycles = 0;
+};
+thread_local SccPolicy t_scc;
+long precision_now() { return t_prec_override ? t_prec_override : g_precision.load(); }
+long refine_now() { return t_refine_override >= 0 ? t_refine_override : g_refine_iters.load(); }
 std::atomic<long> g_mixed_gemm{3};    // FP32 GEMMs of the mixed solve: 0 CUDA cores, 1 TF32, 3 3xTF32 (tcgen05)
 std::atomic<long> g_reduction{1};     // 1: one-stage resident sytrd + ormtr; 2: two-stage sy2sb + sb2st
 std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (16, 32, 64)
@@ -449,7 +466,7 @@ Reduction<T> stage_reduce(Call& k, const char* pre, int n, T* f, T* d, T* e, con
         k.check(ormtr_prepare<T>(n, red.r, n, red.tau, red.nb, red.ow, k.c->arena, k.c->aux, tc), "ormtr prepare");
       if (xq_x && k.ok()) {
         set_identity<T>(n, xq_q, n, k.c->aux);
-        k.check(ormtr_apply<T>(n, n, xq_q, n, red.nb, red.ow, k.c->arena, k.c->aux, tc), "Q formation");
+        k.check(ormtr_apply<T>(n, n, xq_q, n, red.nb, red.ow, k.c->arena, k.c->aux, tc, true), "Q formation");
         GemmDesc<T> p = gemm_problem<T>(n, n, n, T(1), xq_x, xq_ldx, 0, xq_q, n, 0, T(0), xq_m, n, kTriAUpper);
         if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.c->aux), "X Q");
         red.xq = true;
@@ -667,8 +684,9 @@ void solve_factored_mixed(Call& k, int n, double* h, const double* u, int ldu, c
     k.mark("trmm");
   }
   if (k.ok()) convert_mat_f32_to_f64(n, n, tf, n, c, n, k.s);
-  if (k.ok())
-    k.check(refine_generalized(n, h, n, nullptr, 0, u, ldu, c, n, w, (int)g_refine_iters.load(), rw, k.c->arena,
+  // refine_iters 0: plain FP32 vectors (promoted) and the FP64 divide and conquer's eigenvalues, xtb's FP32 SCC mode.
+  if (k.ok() && refine_now() > 0)
+    k.check(refine_generalized(n, h, n, nullptr, 0, u, ldu, c, n, w, (int)refine_now(), rw, k.c->arena,
                                k.s, &tc),
             "refine");
   k.mark("refine");
@@ -677,8 +695,8 @@ void solve_factored_mixed(Call& k, int n, double* h, const double* u, int ldu, c
 // Generalized solve given the factorization (u = U, x = U^-1): h consumed, c <- C, w <- eigenvalues.
 void core_sygvd_factored(Call& k, int n, double* h, const double* u, int ldu, const double* x, int ldx, double* c,
                          double* w) {
-  t_plan = plan_for(n, (int)g_precision.load());
-  if (g_precision.load() == 32) solve_factored_mixed(k, n, h, u, ldu, x, ldx, c, w);
+  t_plan = plan_for(n, (int)precision_now());
+  if (precision_now() == 32) solve_factored_mixed(k, n, h, u, ldu, x, ldx, c, w);
   else solve_factored_fp64(k, n, h, x, ldx, c, w);
 }
 
@@ -985,8 +1003,8 @@ void sygvd_device_body(Call& k, int n, double* a, int lda, double* b, int ldb, d
 
 int sygvd_device(Context* c, cudaStream_t s, int n, double* a, int lda, double* b, int ldb, double* w) {
   const std::vector<long long> key = {1, n, (long long)(uintptr_t)a, lda, (long long)(uintptr_t)b, ldb,
-                                      (long long)(uintptr_t)w, (long long)(uintptr_t)s, g_precision.load(),
-                                      g_refine_iters.load(), plan_for(n, (int)g_precision.load()).sig()};
+                                      (long long)(uintptr_t)w, (long long)(uintptr_t)s, precision_now(),
+                                      refine_now(), plan_for(n, (int)precision_now()).sig()};
   DeviceStatus st{};
   const int code = run_graphed(c, s, key, &st, [&](Call& k) { sygvd_device_body(k, n, a, lda, b, ldb, w); });
   return info_of(code, st, n);
@@ -1077,9 +1095,12 @@ int run_batch(int count, const int* n, int* info, const std::function<int(int)>&
   const std::vector<std::vector<int>> lists = lpt_assign(count, n, nw);
   std::vector<int> inf(count, 0);
   std::vector<std::string> msg(count);
+  const long prec_o = t_prec_override, refine_o = t_refine_override;  // the caller's SCC policy applies to its batch
   pool().run(nw, [&](int wk) {
     const cudaError_t e = cudaSetDevice(dev);
     t_batch_workers = nw;
+    t_prec_override = prec_o;
+    t_refine_override = refine_o;
     for (int i : lists[wk]) {
       if (e != cudaSuccess) {
         inf[i] = -1000 - (int)e;
@@ -1287,8 +1308,8 @@ int xtb_dsygvd_factored_device(int n, double* a, int lda, const double* u, int l
   if (!c) return t_state.last_code;
   const std::vector<long long> key = {4, n, (long long)(uintptr_t)a, lda, (long long)(uintptr_t)u, ldu,
                                       (long long)(uintptr_t)x, ldx, (long long)(uintptr_t)w,
-                                      (long long)(uintptr_t)stream, g_precision.load(), g_refine_iters.load(),
-                                      plan_for(n, (int)g_precision.load()).sig()};
+                                      (long long)(uintptr_t)stream, precision_now(), refine_now(),
+                                      plan_for(n, (int)precision_now()).sig()};
   DeviceStatus st{};
   const int code = run_graphed(c, (cudaStream_t)stream, key, &st, [&](Call& k) {
     double* dh = k.dev<double>("dv.F", (size_t)n * n);
@@ -1400,11 +1421,12 @@ int xtb_gpu_autotune(int n, int precision, void* stream) {
   // Candidates, one coordinate at a time: the reduction (one stage with the resident kernel on all / 3/4 / 1/2 of the
   // SMs; two stages with band width 16 / 32 / 64), then ormtr's block size for the one-stage winner, then the FP32
   // GEMM engine of the mixed path, then the FP64 engine of the large GEMMs (DMMA or int8 Ozaki).
-  const long prec0 = g_precision.load();
-  g_precision = precision;
+  // The candidates run at `precision` on this thread only (the process-wide option is left alone).
+  const long prec0 = t_prec_override;
+  t_prec_override = precision;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
-    g_precision = prec0;
+    t_prec_override = prec0;
     record(-1000, "autotune: event creation failed");
     return -1000;
   }
@@ -1477,7 +1499,7 @@ int xtb_gpu_autotune(int n, int precision, void* stream) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  g_precision = prec0;
+  t_prec_override = prec0;
   if (best.ms < 0.0) {
     record(-3, "autotune: no candidate plan completed");
     return -3;
@@ -1658,7 +1680,7 @@ int xtb_gpu_set_option(const char* name, long value) {
     return 0;
   }
   if (!std::strcmp(name, "refine_iters")) {
-    if (value < 1 || value > 10) return -2;
+    if (value < 0 || value > 10) return -2;
     g_refine_iters = value;
     return 0;
   }
@@ -1714,6 +1736,54 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "test_barrier_stall")) return g_test_stall;
   if (!std::strcmp(name, "backtransform")) return g_backtransform;
   return -1;
+}
+
+int xtb_gpu_scc_set_precision(double fp32_rmsq, int fp32_maxiter, int fp32_refine) {
+  if (!(fp32_rmsq >= 0.0) || !std::isfinite(fp32_rmsq)) return -1;
+  if (fp32_maxiter < 1) return -2;
+  if (fp32_refine != 0 && fp32_refine != 1) return -3;
+  SccPolicy& p = t_scc;
+  p = SccPolicy();
+  p.on = fp32_rmsq > 0.0;
+  p.rmsq = fp32_rmsq;
+  p.maxiter = fp32_maxiter;
+  p.refine = fp32_refine;
+  t_prec_override = 0;
+  t_refine_override = -1;
+  return 0;
+}
+
+int xtb_gpu_scc_cycle(int cycle, double rmsq) {
+  SccPolicy& p = t_scc;
+  if (!p.on) return (int)precision_now();
+  p.cycles = cycle;
+  int prec;
+  if (p.restarted || p.latched64) {
+    prec = 64;
+  } else if (p.fp32_cycles > 0 && cycle > p.maxiter) {
+    // The run used FP32 and has not converged within fp32_maxiter cycles: the caller reruns it from its start, and
+    // every solve of the rerun is FP64 (a full restart, not a hand-off from the FP32-perturbed state).
+    p.restarted = true;
+    t_prec_override = 64;
+    t_refine_override = -1;
+    return 0;
+  } else if (cycle <= 1 || !(rmsq >= 0.0) || rmsq > p.rmsq) {
+    prec = 32;
+    p.fp32_cycles++;
+  } else {
+    p.latched64 = true;  // once the density change is small, FP64 to convergence
+    prec = 64;
+  }
+  t_prec_override = prec;
+  t_refine_override = prec == 32 ? (p.refine ? g_refine_iters.load() : 0) : -1;
+  return prec;
+}
+
+int xtb_gpu_scc_report(int* fp32_cycles, int* restarted, int* precision) {
+  if (fp32_cycles) *fp32_cycles = t_scc.fp32_cycles;
+  if (restarted) *restarted = t_scc.restarted ? 1 : 0;
+  if (precision) *precision = (int)precision_now();
+  return t_scc.on ? 1 : 0;
 }
 
 int xtb_gpu_set_device(int device) {

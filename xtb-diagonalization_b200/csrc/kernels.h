@@ -178,7 +178,7 @@ cudaError_t ormtr_prepare(int n, const T* a, int lda, const T* tau, int nb, Ormt
                           cudaStream_t s, const TcGemm& tc = TcGemm());
 template <typename T>
 cudaError_t ormtr_apply(int n, int m, T* z, int ldz, int nb, OrmtrWork<T> w, DescArena& arena, cudaStream_t s,
-                        const TcGemm& tc = TcGemm());
+                        const TcGemm& tc = TcGemm(), bool from_identity = false);
 
 // ---------------------------------------------------------------------------------------------------- two-stage
 // Stage 1 (sy2sb.cu): a (n x n, full symmetric, lda) -> band of width b in a's lower triangle and in band storage ab

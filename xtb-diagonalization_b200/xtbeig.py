@@ -61,6 +61,9 @@ def lib():
         _lib.xtb_gpu_stage_ms.restype = C.c_double
         _lib.xtb_gpu_stage_ms.argtypes = [_I]
         _lib.xtb_gpu_launch_count.restype = C.c_longlong
+        _lib.xtb_gpu_scc_set_precision.argtypes = [C.c_double, _I, _I]
+        _lib.xtb_gpu_scc_cycle.argtypes = [_I, C.c_double]
+        _lib.xtb_gpu_scc_report.argtypes = [_P, _P, _P]
     return _lib
 
 
@@ -123,6 +126,26 @@ def stage_times():
     """[(stage, ms)] of the calling thread's last call (with set_option("stage_timing", 1))."""
     L = lib()
     return [(L.xtb_gpu_stage_name(i).decode(), float(L.xtb_gpu_stage_ms(i))) for i in range(L.xtb_gpu_stage_count())]
+
+
+def scc_set_precision(fp32_rmsq: float, fp32_maxiter: int = 160, fp32_refine: int = 0) -> None:
+    """Start an SCC run under the FP32-early / FP64-to-convergence policy of the calling thread
+    (xtb_gpu_scc_set_precision; fp32_rmsq 0 turns it off)."""
+    rc = lib().xtb_gpu_scc_set_precision(float(fp32_rmsq), int(fp32_maxiter), int(fp32_refine))
+    if rc != 0:
+        raise ValueError(f"xtb_gpu_scc_set_precision returned {rc}")
+
+
+def scc_cycle(cycle: int, rmsq: float) -> int:
+    """Precision (32 or 64) of this SCC cycle's solves, or 0 when the caller must rerun the SCC in FP64."""
+    return int(lib().xtb_gpu_scc_cycle(int(cycle), float(rmsq)))
+
+
+def scc_report():
+    """(policy on, FP32 cycles, restarted, precision in effect) of the calling thread."""
+    a, b, c = _I(0), _I(0), _I(0)
+    on = lib().xtb_gpu_scc_report(C.byref(a), C.byref(b), C.byref(c))
+    return bool(on), a.value, bool(b.value), c.value
 
 
 def launch_count() -> int:
