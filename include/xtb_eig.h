@@ -89,6 +89,17 @@ int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, 
 #define XTB_NOALLOC_MAX_N 1792
 int xtb_dsytrd_upper_noalloc(int n, double* a, int lda, double* d, double* e, double* tau, void* stream);
 
+/* The lowest m eigenpairs of H C = S C e (DEVICE pointers, as xtb_dsygvd_device): every eigenvalue goes to w (n), the
+ * eigenvectors of the m smallest to a's first m columns (the rest of a is left as it was), the Cholesky factor to b.
+ * xTB needs the occupied orbitals (plus the partly occupied ones under Fermi smearing) in every SCC cycle and all of
+ * them only after convergence; the reference measures 1.29-1.46x from m = n/2 on its CPU path (LOG.md:300-305).
+ * FP64: the divide and conquer's top merge forms only the m wanted columns (the reference's partial top merge,
+ * scripts/kernels/stedc_partial.c) and the back-transformation runs on m columns.  Precision 32: the FP32 chain forms
+ * every vector as the basis, then only the m lowest pairs (plus a margin of 32) are refined in FP64, 10 n^2 (m + 32)
+ * flops per step instead of 7 n^3; w's entries from m + 32 on are then the FP32 chain's (about 1e-6 accurate).  m = 0
+ * or m = n: all vectors.  Returns info as xtb_dsygvd_device, or -2 for m outside 0..n. */
+int xtb_dsygvd_lowest_device(int n, int m, double* a, int lda, double* b, int ldb, double* w, void* stream);
+
 /* Per-geometry / per-SCC-cycle split of xtb_dsygvd_device, for xTB's loop in which S is fixed per geometry and H
  * changes every cycle (the reference factors S once per geometry, mctc_potrf, and reduces each cycle with the
  * congruence of scripts/kernels/congruence.c:33-52).  xtb_dsygvd_factor_device: b (S's upper triangle, ldb) <- U with

@@ -529,11 +529,11 @@ bool use_xq(Call& k, int n) {
 
 // The C = (X Q) Z step after the tridiagonal eigensolve: waits for the aux stream's X Q, then one GEMM.
 template <typename T>
-void stage_xq_backtransform(Call& k, int n, const T* m, const T* z, T* c, const TcGemm& tc) {
+void stage_xq_backtransform(Call& k, int n, int cols, const T* m, const T* z, T* c, const TcGemm& tc) {
   if (!k.ok()) return;
   k.check(cudaStreamWaitEvent(k.s, k.c->ev_join, 0), "join");
   k.mark("xq_join");
-  GemmDesc<T> p = gemm_problem<T>(n, n, n, T(1), m, n, 0, z, n, 0, T(0), c, n);
+  GemmDesc<T> p = gemm_problem<T>(n, cols, n, T(1), m, n, 0, z, n, 0, T(0), c, n);
   if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "C = (X Q) Z");
   k.mark("backtransform");
 }
@@ -568,7 +568,7 @@ TcGemm tc_engine_refine(Call& k, int n) {
   return tc;
 }
 
-void stage_stedc(Call& k, int n, double* d, double* e, double* z, int ldz) {
+void stage_stedc(Call& k, int n, double* d, double* e, double* z, int ldz, int m_cols = 0) {
   if (!k.ok() || n <= 0) return;
   const size_t wb = stedc_work_bytes(n);
   char* w = k.template dev<char>("stedc.work", wb);
@@ -581,7 +581,7 @@ void stage_stedc(Call& k, int n, double* d, double* e, double* z, int ldz) {
   const size_t hb = (size_t)40 * n * sizeof(int) + (size_t)4 * (n + 8) * sizeof(GemmDesc<double>) + 4096;
   char* h = ready ? nullptr : k.template host<char>("stedc.stage", hb);
   if (!k.ok()) return;
-  k.check(stedc_device(n, d, e, z, ldz, w, wb, plan, !ready, h, hb, k.c->d_status, k.s), "stedc");
+  k.check(stedc_device(n, d, e, z, ldz, w, wb, plan, !ready, h, hb, k.c->d_status, k.s, m_cols), "stedc");
   if (k.ok()) ready = true;
 }
 
@@ -600,7 +600,8 @@ void stage_factor(Call& k, int n, double* u, int ldu, double* x, int ldx) {
 
 // The generalized solve after the factorization (FP64): h (n x n, full symmetric, ld n) is consumed; u = U, x = U^-1
 // (upper, from stage_factor); c (n x n, ld n) receives C; w (n) the eigenvalues.
-void solve_factored_fp64(Call& k, int n, double* h, const double* x, int ldx, double* c, double* w) {
+// mv < n: only the eigenvectors of the mv smallest eigenvalues (c's first mv columns; every eigenvalue in w).
+void solve_factored_fp64(Call& k, int n, double* h, const double* x, int ldx, double* c, double* w, int mv) {
   if (!k.ok() || n <= 0) return;
   double* t = k.template dev<double>("gv.T", (size_t)n * n);
   double* hp = k.template dev<double>("gv.Hp", (size_t)n * n);
@@ -621,15 +622,15 @@ void solve_factored_fp64(Call& k, int n, double* h, const double* x, int ldx, do
   double* mx = xq ? k.template dev<double>("gv.M", (size_t)n * n) : nullptr;
   if (!k.ok()) return;
   const Reduction<double> red = stage_reduce<double>(k, "gv.", n, h, w, e, tc, true, xq ? x : nullptr, ldx, qx, mx);
-  stage_stedc(k, n, w, e, z, n);
+  stage_stedc(k, n, w, e, z, n, mv);
   k.mark("stedc");
   if (red.xq) {
-    stage_xq_backtransform<double>(k, n, mx, z, c, tc);
+    stage_xq_backtransform<double>(k, n, mv, mx, z, c, tc);
     return;
   }
-  stage_backtransform<double>(k, "gv.", n, n, red, z, n, tc);
+  stage_backtransform<double>(k, "gv.", n, mv, red, z, n, tc);
   // C = X Z (X upper).
-  p = gemm_problem<double>(n, n, n, 1.0, x, ldx, 0, z, n, 0, 0.0, c, n, kTriAUpper);
+  p = gemm_problem<double>(n, mv, n, 1.0, x, ldx, 0, z, n, 0, 0.0, c, n, kTriAUpper);
   if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "back-transform");
   k.mark("trmm");
 }
@@ -637,14 +638,20 @@ void solve_factored_fp64(Call& k, int n, double* h, const double* x, int ldx, do
 // Mixed precision after the factorization: the reduction chain in FP32 (congruence, reduction, back-transformations;
 // the tridiagonal eigensolve in FP64), then FP64 Ogita-Aishima refinement on the FP64 pair (H, S = U^T U), with
 // C^T S C formed as (U C)^T (U C).  h is kept intact here.
+// mv < n: the FP32 chain forms every vector (the basis of the refinement), then only the mv lowest eigenpairs (and
+// a margin) are refined in FP64 (refine_lowest); c's first mv columns and w's first mv entries are the result, the
+// rest of w holds the FP32 chain's eigenvalues.
 void solve_factored_mixed(Call& k, int n, double* h, const double* u, int ldu, const double* x, int ldx, double* c,
-                          double* w) {
+                          double* w, int mv) {
   if (!k.ok() || n <= 0) return;
   const size_t nn = (size_t)n * n;
+  const bool lowest = mv < n && refine_lowest_mr(n, mv) < n;
   double* z = k.template dev<double>("gv.Z", nn);
   double* e = k.template dev<double>("gv.e", (size_t)n);
   float* f = k.template dev<float>("mx.f32", 5 * nn + 2 * (size_t)n);
-  double* rw = k.template dev<double>("mx.refine", refine_work_elems(n));
+  double* rw = k.template dev<double>("mx.refine", lowest ? std::max(refine_lowest_work_elems(n, mv),
+                                                                     refine_work_elems(n))
+                                                          : refine_work_elems(n));
   if (!k.ok()) return;
   float* xf = f;
   float* hf = xf + nn;
@@ -676,7 +683,7 @@ void solve_factored_mixed(Call& k, int n, double* h, const double* u, int ldu, c
   k.mark("stedc");
   if (k.ok()) convert_mat_f64_to_f32(n, n, z, n, zf, n, k.s);
   if (red.xq) {
-    stage_xq_backtransform<float>(k, n, mxf, zf, tf, tc);
+    stage_xq_backtransform<float>(k, n, n, mxf, zf, tf, tc);
   } else {
     stage_backtransform<float>(k, "mx.", n, n, red, zf, n, tc);
     p = gemm_problem<float>(n, n, n, 1.f, xf, n, 0, zf, n, 0, 0.f, tf, n, kTriAUpper);
@@ -685,7 +692,10 @@ void solve_factored_mixed(Call& k, int n, double* h, const double* u, int ldu, c
   }
   if (k.ok()) convert_mat_f32_to_f64(n, n, tf, n, c, n, k.s);
   // refine_iters 0: plain FP32 vectors (promoted) and the FP64 divide and conquer's eigenvalues, xtb's FP32 SCC mode.
-  if (k.ok() && refine_now() > 0)
+  if (k.ok() && refine_now() > 0 && lowest)
+    k.check(refine_lowest(n, mv, h, n, u, ldu, c, n, w, (int)refine_now(), rw, k.c->arena, k.s, &tc),
+            "refine (lowest)");
+  else if (k.ok() && refine_now() > 0)
     k.check(refine_generalized(n, h, n, nullptr, 0, u, ldu, c, n, w, (int)refine_now(), rw, k.c->arena,
                                k.s, &tc),
             "refine");
@@ -694,19 +704,20 @@ void solve_factored_mixed(Call& k, int n, double* h, const double* u, int ldu, c
 
 // Generalized solve given the factorization (u = U, x = U^-1): h consumed, c <- C, w <- eigenvalues.
 void core_sygvd_factored(Call& k, int n, double* h, const double* u, int ldu, const double* x, int ldx, double* c,
-                         double* w) {
+                         double* w, int m = 0) {
   t_plan = plan_for(n, (int)precision_now());
-  if (precision_now() == 32) solve_factored_mixed(k, n, h, u, ldu, x, ldx, c, w);
-  else solve_factored_fp64(k, n, h, x, ldx, c, w);
+  const int mv = (m > 0 && m < n) ? m : n;
+  if (precision_now() == 32) solve_factored_mixed(k, n, h, u, ldu, x, ldx, c, w, mv);
+  else solve_factored_fp64(k, n, h, x, ldx, c, w, mv);
 }
 
 // The generalized core on device buffers: h (n x n, full symmetric, ld n) is consumed; u (n x n, ld n) holds B's upper
 // triangle on entry and U on exit; c (n x n, ld n) receives C; w (n) the eigenvalues.
-void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w) {
+void core_sygvd(Call& k, int n, double* h, double* u, double* c, double* w, int m = 0) {
   if (!k.ok() || n <= 0) return;
   double* x = k.template dev<double>("gv.X", (size_t)n * n);
   stage_factor(k, n, u, n, x, n);
-  core_sygvd_factored(k, n, h, u, n, x, n, c, w);
+  core_sygvd_factored(k, n, h, u, n, x, n, c, w, m);
 }
 
 // Standard problem on device buffers: f (n x n full symmetric, ld n) consumed; z (n x n) eigenvectors; w eigenvalues.
@@ -986,7 +997,9 @@ int sygvd_host(char jz, char ul, int n, double* a, int lda, double* b, int ldb, 
 }
 
 // Device-pointer dsygvd body (upper triangles in a and b, ld lda/ldb): a <- C, b <- U, w <- eigenvalues.
-void sygvd_device_body(Call& k, int n, double* a, int lda, double* b, int ldb, double* w) {
+// m < n: only the eigenvectors of the m smallest eigenvalues are written (a's first m columns).
+void sygvd_device_body(Call& k, int n, double* a, int lda, double* b, int ldb, double* w, int m = 0) {
+  const int mv = (m > 0 && m < n) ? m : n;
   double* dh = k.dev<double>("dv.F", (size_t)n * n);
   double* du = k.dev<double>("dv.U", (size_t)n * n);
   double* dc = k.dev<double>("dv.C", (size_t)n * n);
@@ -994,19 +1007,19 @@ void sygvd_device_body(Call& k, int n, double* a, int lda, double* b, int ldb, d
     symmetrize_upper<double>(n, a, lda, dh, n, k.s);
     copy_matrix<double>(n, n, b, ldb, du, n, k.s);
   }
-  core_sygvd(k, n, dh, du, dc, w);
+  core_sygvd(k, n, dh, du, dc, w, mv);
   if (k.ok()) {
-    copy_matrix<double>(n, n, dc, n, a, lda, k.s);
+    copy_matrix<double>(n, mv, dc, n, a, lda, k.s);
     copy_matrix<double>(n, n, du, n, b, ldb, k.s);
   }
 }
 
-int sygvd_device(Context* c, cudaStream_t s, int n, double* a, int lda, double* b, int ldb, double* w) {
+int sygvd_device(Context* c, cudaStream_t s, int n, double* a, int lda, double* b, int ldb, double* w, int m = 0) {
   const std::vector<long long> key = {1, n, (long long)(uintptr_t)a, lda, (long long)(uintptr_t)b, ldb,
                                       (long long)(uintptr_t)w, (long long)(uintptr_t)s, precision_now(),
-                                      refine_now(), plan_for(n, (int)precision_now()).sig()};
+                                      refine_now(), plan_for(n, (int)precision_now()).sig(), m};
   DeviceStatus st{};
-  const int code = run_graphed(c, s, key, &st, [&](Call& k) { sygvd_device_body(k, n, a, lda, b, ldb, w); });
+  const int code = run_graphed(c, s, key, &st, [&](Call& k) { sygvd_device_body(k, n, a, lda, b, ldb, w, m); });
   return info_of(code, st, n);
 }
 
@@ -1281,6 +1294,17 @@ int xtb_dsygvd_device(int n, double* a, int lda, double* b, int ldb, double* w, 
   Context* c = context();
   if (!c) return t_state.last_code;
   return sygvd_device(c, (cudaStream_t)stream, n, a, lda, b, ldb, w);
+}
+
+int xtb_dsygvd_lowest_device(int n, int m, double* a, int lda, double* b, int ldb, double* w, void* stream) {
+  if (n < 0) return -1;
+  if (m < 0 || m > n) return -2;
+  if (lda < std::max(1, n)) return -4;
+  if (ldb < std::max(1, n)) return -6;
+  if (n == 0) return 0;
+  Context* c = context();
+  if (!c) return t_state.last_code;
+  return sygvd_device(c, (cudaStream_t)stream, n, a, lda, b, ldb, w, m == 0 ? n : m);
 }
 
 int xtb_dsygvd_factor_device(int n, double* b, int ldb, double* x, int ldx, void* stream) {

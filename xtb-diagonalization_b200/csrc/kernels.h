@@ -214,8 +214,11 @@ size_t stedc_work_bytes(int n);
 // `plan` (stedc_plan_bytes(n)) holds the per-level plan for this n; upload_plan copies it from hstage first (needed
 // once per plan buffer).
 size_t stedc_plan_bytes(int n);
+// m_cols < n: every eigenvalue, but only the eigenvectors of the m_cols smallest (z's first m_cols columns); the top
+// merge forms only those columns.
 cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* work, size_t work_bytes, void* plan,
-                         bool upload_plan, void* hstage, size_t hstage_bytes, DeviceStatus* st, cudaStream_t s);
+                         bool upload_plan, void* hstage, size_t hstage_bytes, DeviceStatus* st, cudaStream_t s,
+                         int m_cols = 0);
 
 // ---------------------------------------------------------------------------------------------------- potrf / trtri
 // S = U^T U (upper, in place) and X = U^-1 (upper, strict lower part zero) in one recursion; t: n x n scratch (ld n).
@@ -242,6 +245,14 @@ size_t refine_ozaki_bytes(int n);
 cudaError_t refine_generalized(int n, const double* h, int ldh, const double* s, int lds, const double* u, int ldu,
                                double* c, int ldc, double* w, int iters, double* work, DescArena& arena,
                                cudaStream_t st, const TcGemm* tc = nullptr);
+// The lowest m eigenpairs only: c (n x n, ldc) holds every approximate eigenvector in ascending order and w their
+// approximate eigenvalues; refine_lowest_mr(n, m) >= m leading columns are refined against the whole basis (the others
+// stay as they are) with u the upper Cholesky factor of S, and c(:, 0:mr), w(0:mr) rewritten in ascending order.
+// work: refine_lowest_work_elems(n, m) doubles.
+int refine_lowest_mr(int n, int m);
+size_t refine_lowest_work_elems(int n, int m);
+cudaError_t refine_lowest(int n, int m, const double* h, int ldh, const double* u, int ldu, double* c, int ldc,
+                          double* w, int iters, double* work, DescArena& arena, cudaStream_t st, const TcGemm* tc);
 
 // ---------------------------------------------------------------------------------------------------- helpers
 // Stage nprob descriptors through the arena (tile grid and tile_begin filled in from M, N) and launch one grouped GEMM.

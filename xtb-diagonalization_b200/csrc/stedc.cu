@@ -564,6 +564,34 @@ __global__ void dc_vectors_kernel(DcBufs B) {
   for (int i = lane; i < K; i += 32) up[B.slotOf[s + i]] = (B.zh[s + i] / dcol[i]) * inv;
 }
 
+// ------------------------------------------------------------------------------------------------ partial top merge
+
+// The top merge when only the eigenvectors of the m_cols smallest eigenvalues are wanted: root j lands at output
+// position j + #(deflated values below it), so the roots that land below m_cols are a prefix 0 .. Km-1 of the
+// ascending roots.  The merge GEMMs' N (root columns) is cut to Km before they run; every eigenvalue is still formed.
+// One CTA; the top level has one merge.
+__global__ void __launch_bounds__(1024) dc_partial_kernel(DcBufs B, int m_cols) {
+  DC_RETURN_IF_FAILED(B)
+  __shared__ int red[32];
+  const MergeDesc md = B.merges[0];
+  const MergeInfo inf = B.info[0];
+  const int s = md.s, n = md.n1 + md.n2, K = inf.K, nd = n - K;
+  const double* lam = B.lam + s;
+  const double* dv = B.dval + s;
+  int below = 0;
+  for (int j = threadIdx.x; j < K; j += blockDim.x) {
+    const double x = lam[j];
+    int c = 0;
+    for (int t = 0; t < nd; ++t) c += okey(dv[t]) < okey(x);
+    below += (j + c < m_cols) ? 1 : 0;
+  }
+  below = block_sum(below, red);
+  if (threadIdx.x == 0) {
+    B.gdesc[0].N = below;
+    B.gdesc[1].N = below;
+  }
+}
+
 // ------------------------------------------------------------------------------------------------ final order
 
 // grid (merges, column groups): rank of every root and deflated value in the merged ascending order; the CTAs of a
@@ -597,13 +625,13 @@ __global__ void dc_order_kernel(DcBufs B, double* dnext) {
 }
 
 // grid (merges, columns): copy each output column into the next level's eigenvector matrix, one column per CTA with a
-// grid-stride loop over the merge's columns.
-__global__ void dc_copy_kernel(DcBufs B) {
+// grid-stride loop over the merge's columns; columns from col_limit on are not wanted (partial top merge).
+__global__ void dc_copy_kernel(DcBufs B, int col_limit) {
   DC_RETURN_IF_FAILED(B)
   const int mi = blockIdx.x;
   const MergeDesc md = B.merges[mi];
   const MergeInfo inf = B.info[mi];
-  const int s = md.s, n = md.n1 + md.n2, K = inf.K;
+  const int s = md.s, n = min(md.n1 + md.n2, col_limit), K = inf.K;
   const size_t ld = B.ld;
   // One column per CTA (while the grid allows): enough CTAs in flight to cover the copy's memory latency.
   for (int c = blockIdx.y; c < n; c += gridDim.y) {
@@ -614,11 +642,11 @@ __global__ void dc_copy_kernel(DcBufs B) {
   }
 }
 
-__global__ void dc_finish_kernel(int n, const double* dd, const double* scale, double* d_out, const double* q,
-                                 int ldq, double* z, int ldz) {
+__global__ void dc_finish_kernel(int n, int m_cols, const double* dd, const double* scale, double* d_out,
+                                 const double* q, int ldq, double* z, int ldz) {
   const double sc = scale[0] > 0.0 ? scale[0] : 1.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d_out[i] = dd[i] * sc;
-  const size_t total = (size_t)n * n;
+  const size_t total = (size_t)n * m_cols;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(idx % n), j = (int)(idx / n);
     z[i + (size_t)j * ldz] = q[i + (size_t)j * ldq];
@@ -676,8 +704,10 @@ size_t stedc_plan_bytes(int n) {
 }
 
 cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* work, size_t work_bytes, void* plan,
-                         bool upload_plan, void* hstage, size_t hstage_bytes, DeviceStatus* st, cudaStream_t s) {
+                         bool upload_plan, void* hstage, size_t hstage_bytes, DeviceStatus* st, cudaStream_t s,
+                         int m_cols) {
   if (n <= 0) return cudaSuccess;
+  if (m_cols <= 0 || m_cols > n) m_cols = n;
   if (work_bytes < stedc_work_bytes(n)) return cudaErrorInvalidValue;
   char* p = reinterpret_cast<char*>(work);
   char* pp = reinterpret_cast<char*>(plan);
@@ -809,16 +839,21 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
     dc_secular_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();
     dc_zhat_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();
     dc_vectors_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();
+    const bool partial = l == L - 1 && m_cols < n;  // the top merge forms only the wanted columns
+    if (partial) {
+      dc_partial_kernel<<<1, 1024, 0, s>>>(B, m_cols); note_launches();
+    }
     gemm_grouped_launch<double>(B.gdesc, 2 * nm, tiles[l], s);
     dc_order_kernel<<<dim3(nm, (maxn + 255) / 256), 256, 0, s>>>(B, dnext); note_launches();
-    dc_copy_kernel<<<dim3(nm, std::min(maxn, 65535)), 256, 0, s>>>(B); note_launches();
+    dc_copy_kernel<<<dim3(nm, std::min(partial ? m_cols : maxn, 65535)), 256, 0, s>>>(B, partial ? m_cols : n);
+    note_launches();
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     // Next level reads (dd, Qa) = (dnext, Qb); the old Qa becomes the next output buffer.
     std::swap(B.Qa, B.Qb);
     std::swap(B.dd, dnext);
   }
-  dc_finish_kernel<<<1024, 256, 0, s>>>(n, B.dd, B.scale, d, B.Qa, n, z, ldz); note_launches();
+  dc_finish_kernel<<<1024, 256, 0, s>>>(n, m_cols, B.dd, B.scale, d, B.Qa, n, z, ldz); note_launches();
   return cudaGetLastError();
 }
 

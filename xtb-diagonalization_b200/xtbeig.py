@@ -61,6 +61,7 @@ def lib():
         _lib.xtb_gpu_stage_ms.restype = C.c_double
         _lib.xtb_gpu_stage_ms.argtypes = [_I]
         _lib.xtb_gpu_launch_count.restype = C.c_longlong
+        _lib.xtb_dsygvd_lowest_device.argtypes = [_I, _I, _P, _I, _P, _I, _P, _P]
         _lib.xtb_gpu_scc_set_precision.argtypes = [C.c_double, _I, _I]
         _lib.xtb_gpu_scc_cycle.argtypes = [_I, C.c_double]
         _lib.xtb_gpu_scc_report.argtypes = [_P, _P, _P]
@@ -248,6 +249,29 @@ def dsygvd_device(n, a_ptr, lda, b_ptr, ldb, w_ptr, stream=0) -> int:
     """Device-pointer solve (column-major device buffers, e.g. torch tensors' data_ptr())."""
     return int(lib().xtb_dsygvd_device(int(n), _P(a_ptr), int(lda), _P(b_ptr), int(ldb), _P(w_ptr),
                                        _P(stream) if stream else None))
+
+
+def dsygvd_lowest_device(n, m, a_ptr, lda, b_ptr, ldb, w_ptr, stream=0) -> int:
+    """xtb_dsygvd_lowest_device: every eigenvalue and the eigenvectors of the m smallest (device buffers)."""
+    return int(lib().xtb_dsygvd_lowest_device(int(n), int(m), _P(a_ptr), int(lda), _P(b_ptr), int(ldb), _P(w_ptr),
+                                              _P(stream) if stream else None))
+
+
+def dsygvd_lowest(h, s, m):
+    """Host convenience over xtb_dsygvd_lowest_device (torch moves the arrays): returns (w, C[:, :m], info); m = 0
+    means every vector."""
+    import torch
+
+    n = np.asarray(h).shape[0]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    H = torch.from_numpy(np.ascontiguousarray(np.asfortranarray(h, dtype=np.float64).T)).to(dev)
+    S = torch.from_numpy(np.ascontiguousarray(np.asfortranarray(s, dtype=np.float64).T)).to(dev)
+    W = torch.zeros(max(n, 1), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    info = dsygvd_lowest_device(n, m, H.data_ptr(), max(n, 1), S.data_ptr(), max(n, 1), W.data_ptr())
+    torch.cuda.synchronize(dev)
+    c = H.cpu().numpy().T
+    return W.cpu().numpy()[:n], np.asfortranarray(c[:, : (m if m else n)]), info
 
 
 def dsygvd_refine_device(n, h_ptr, ldh, s_ptr, lds, c_ptr, ldc, w_ptr, iters=2, stream=0) -> int:
