@@ -77,7 +77,7 @@ def test_config3_two_stage_fp64_n1788(options, config3, b):
     _check(h, s, lam, w_ref, c_ref, w, c, 1e-12)
 
 
-@pytest.mark.parametrize("b", [32, 64])
+@pytest.mark.parametrize("b", [32, 64, 128])
 def test_config3_two_stage_mixed_n1788(options, config3, b):
     options.set_option("reduction", 2)
     options.set_option("band_width", b)

@@ -131,3 +131,26 @@ def test_dgemm_matches_fp64(xe, ta, tb, mnk, engine):
         xe.set_option("dgemm_engine", old)
     bound = 2 * (k + 2) * 2.0 ** -53 * absprod + 1e-300
     assert bool(((out - ref).abs() <= bound).all())
+
+
+@pytest.mark.parametrize("ta", [0, 1])
+@pytest.mark.parametrize("tb", [0, 1])
+@pytest.mark.parametrize("mnk", [(1, 1, 1), (31, 33, 17), (127, 129, 65), (200, 64, 300), (300, 257, 1000)])
+@pytest.mark.parametrize("passes", [11, 13])
+def test_sgemm_bf16_matches_fp64(xe, ta, tb, mnk, passes):
+    """BF16 operands on kind::f16 (FP32 accumulation): passes 11 rounds each operand to BF16 (8-bit mantissa),
+    bound 4 (2^-8 + k 2^-24) |op(A)| |op(B)|; passes 13 keeps hi*hi + hi*lo + lo*hi of a two-piece BF16 split,
+    bound 4 (2^-16 + k 2^-24).  The operands are written K-major by the split pass whatever their storage, so all four
+    transpose combinations run the same tensor-core layout."""
+    m, n, k = mnk
+    out, ref, absprod = _run(xe, ta, tb, m, n, k, 1.0, 0.0, passes, seed=m * 5 + n + k + 10 * ta + 20 * tb + passes)
+    rel = 2.0 ** -8 if passes == 11 else 2.0 ** -16
+    bound = 4 * (rel + k * 2.0 ** -24) * absprod + 1e-30
+    err = (out - ref).abs()
+    assert bool((err <= bound).all()), float((err / bound).max())
+
+
+def test_sgemm_bf16_alpha_beta_and_padding(xe):
+    out, ref, absprod = _run(xe, 0, 1, 129, 130, 131, -0.75, 0.5, 13, seed=4, pad=5)
+    bound = 4 * (2.0 ** -16 + 131 * 2.0 ** -24) * absprod + 1e-30
+    assert bool(((out - ref).abs() <= bound).all())

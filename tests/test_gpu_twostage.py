@@ -82,14 +82,16 @@ def test_config2_generalized_n1204_two_stage(two):
     assert metrics.density_error(c, c_ref, metrics.aufbau(1204, 602)) <= 1e-9
 
 
+@pytest.mark.parametrize("b", [32, 128])
 @pytest.mark.parametrize("n", [130, 412])
-def test_mixed_two_stage(two, n):
+def test_mixed_two_stage(two, n, b):
     """Mixed precision through the two-stage reduction.  Its trailing updates run as 3xTF32 tensor-core GEMMs, whose
     operand representation (about 2^-21 per product against FP32's 2^-24) compounds over the panels, so the FP32
     vectors start about ten times less accurate than the one-stage path's.  Two refinement steps still meet the
     mixed path's accuracy targets (eigenvalues <= 1e-10 Eh, density <= 1e-9); S-orthogonality lands near 1e-9 at n = 130, so its
     bar here is 5e-9."""
     two.set_option("precision", 32)
+    two.set_option("band_width", b)
     h, s, lam = inputs.generalized(n, seed=70 + n)
     w_ref, c_ref = lapack.sygvd_chain(h, s)
     w, c, u, info = two.dsygvd(h, s)
@@ -106,3 +108,22 @@ def test_two_stage_repeatable_bits(two):
     w1, z1, _ = two.dsyevd(a)
     w2, z2, _ = two.dsyevd(a)
     assert np.array_equal(w1, w2) and np.array_equal(z1, z2)
+
+
+@pytest.mark.parametrize("n", [3, 100, 129, 130, 257, 300])
+def test_band_width_128_fp32_chain(two, n):
+    """Band width 128 (the widest of the reference's choices for large n, SBROptions.swift:73-82) on the FP32 chain,
+    whose panel and bulge-chase blocks fit in shared memory at this width; FP64 at b = 128 does not fit and the plan
+    falls back to the one-stage reduction (same bars)."""
+    two.set_option("band_width", 128)
+    h, s, lam = inputs.generalized(n, seed=80 + n)
+    w_ref, c_ref = lapack.sygvd_chain(h, s)
+    for precision in (32, 64):
+        two.set_option("precision", precision)
+        w, c, u, info = two.dsygvd(h, s)
+        assert info == 0
+        assert np.max(np.abs(w - lam)) < 1e-10 and np.max(np.abs(w - w_ref)) < 1e-10
+        assert metrics.backward_error(h, s, w, c) < 10
+        assert metrics.s_orthogonality(s, c) < (1e-12 if precision == 64 else 5e-9)
+        if n >= 2:
+            assert metrics.density_error(c, c_ref, metrics.aufbau(n, n // 2)) < 1e-9

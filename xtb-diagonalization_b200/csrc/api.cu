@@ -53,7 +53,7 @@ long precision_now() { return t_prec_override ? t_prec_override : g_precision.lo
 long refine_now() { return t_refine_override >= 0 ? t_refine_override : g_refine_iters.load(); }
 std::atomic<long> g_mixed_gemm{3};    // FP32 GEMMs of the mixed solve: 0 CUDA cores, 1 TF32, 3 3xTF32 (tcgen05)
 std::atomic<long> g_reduction{1};     // 1: one-stage resident sytrd + ormtr; 2: two-stage sy2sb + sb2st
-std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (16, 32, 64)
+std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (16, 32, 64, 128)
 std::atomic<long> g_autotune{0};      // 1: solves use the autotuned plan nearest their size (xtb_gpu_autotune)
 std::atomic<long> g_batch_grid{1};    // 1: batch workers size each resident reduction's grid to its matrix
 std::atomic<long> g_dgemm_engine{1};  // FP64 GEMMs: 0 DMMA, 1 Ozaki (int8 tcgen05) where eligible, 2 Ozaki always
@@ -1382,7 +1382,7 @@ int xtb_sgemm_tc_device(int transa, int transb, int m, int n, int k_, float alph
   if (lda < std::max(1, transa ? k_ : m)) return -8;
   if (ldb < std::max(1, transb ? n : k_)) return -10;
   if (ldc < std::max(1, m)) return -13;
-  if (passes != 1 && passes != 3) return -14;
+  if (passes != 1 && passes != 3 && passes != 11 && passes != 13) return -14;
   if (m == 0 || n == 0) return 0;
   Context* c0 = context();
   if (!c0) return t_state.last_code;
@@ -1494,8 +1494,9 @@ int xtb_gpu_autotune(int n, int precision, void* stream) {
     p.sytrd_grid = g;
     consider(p);
   }
-  for (int b : {16, 32, 64}) {
-    if (!sy2sb_supported(n, b, c->max_smem, 8) || !sb2st_supported(n, b, c->max_smem, 8)) continue;
+  for (int b : {16, 32, 64, 128}) {
+    const int eb = precision == 32 ? 4 : 8;
+    if (!sy2sb_supported(n, b, c->max_smem, eb) || !sb2st_supported(n, b, c->max_smem, eb)) continue;
     Plan p = base;
     p.reduction = 2;
     p.band = b;
@@ -1709,7 +1710,7 @@ int xtb_gpu_set_option(const char* name, long value) {
     return 0;
   }
   if (!std::strcmp(name, "mixed_gemm")) {
-    if (value != 0 && value != 1 && value != 3) return -2;
+    if (value != 0 && value != 1 && value != 3 && value != 11 && value != 13) return -2;
     g_mixed_gemm = value;
     return 0;
   }
@@ -1719,7 +1720,7 @@ int xtb_gpu_set_option(const char* name, long value) {
     return 0;
   }
   if (!std::strcmp(name, "band_width")) {
-    if (value != 16 && value != 32 && value != 64) return -2;
+    if (value != 16 && value != 32 && value != 64 && value != 128) return -2;
     g_band_width = value;
     return 0;
   }

@@ -163,12 +163,17 @@ __global__ void __launch_bounds__(kChaseThreads, 1) sb2st_kernel(const __grid_co
 #define AB(i, j) colp[(j) - c][(i) - (j)]
         // Householder vector from column c, rows rs .. re-1 (warp 0).
         if (warp == 0) {
-          T x0 = T(0), x1 = T(0);
-          if (lane < len) x0 = AB(rs + lane, c);
-          if (BW > 32 && lane + 32 < len) x1 = AB(rs + lane + 32, c);
-          T sq = (lane >= 1 && lane < len ? x0 * x0 : T(0)) + (lane + 32 < len ? x1 * x1 : T(0));
+          constexpr int NX = (BW + 31) / 32;  // elements of the column per lane
+          T xs[NX];
+          T sq = T(0);
+#pragma unroll
+          for (int q = 0; q < NX; ++q) {
+            const int r = lane + 32 * q;
+            xs[q] = r < len ? AB(rs + r, c) : T(0);
+            if (r >= 1 && r < len) sq += xs[q] * xs[q];
+          }
           sq = warp_sum(sq);
-          const T alpha = __shfl_sync(0xffffffffu, x0, 0);
+          const T alpha = __shfl_sync(0xffffffffu, xs[0], 0);
           T beta = alpha, tau = T(0), scale = T(0);
           if (sq > T(0)) {
             const T nrm = sqrt(alpha * alpha + sq);
@@ -177,17 +182,15 @@ __global__ void __launch_bounds__(kChaseThreads, 1) sb2st_kernel(const __grid_co
             scale = T(1) / (alpha - beta);
           }
           const T rt = sqrt(tau);
-          if (lane < len) {
-            const T wv = lane == 0 ? rt : rt * scale * x0;
-            s_w[lane] = wv;
-            p.w2[(size_t)(rs + lane) + (size_t)s * n] = wv;
-            AB(rs + lane, c) = lane == 0 ? beta : T(0);
-          }
-          if (BW > 32 && lane + 32 < len) {
-            const T wv = rt * scale * x1;
-            s_w[lane + 32] = wv;
-            p.w2[(size_t)(rs + lane + 32) + (size_t)s * n] = wv;
-            AB(rs + lane + 32, c) = T(0);
+#pragma unroll
+          for (int q = 0; q < NX; ++q) {
+            const int r = lane + 32 * q;
+            if (r < len) {
+              const T wv = r == 0 ? rt : rt * scale * xs[q];
+              s_w[r] = wv;
+              p.w2[(size_t)(rs + r) + (size_t)s * n] = wv;
+              AB(rs + r, c) = r == 0 ? beta : T(0);
+            }
           }
           if (lane == 0) s_skip = tau == T(0);
         }
@@ -504,12 +507,14 @@ std::vector<Q2Block> q2_blocks(int n, int b) {
 }  // namespace
 
 bool sb2st_supported(int n, int b, size_t max_smem, int elem_bytes) {
-  if (b != 16 && b != 32 && b != 64) return false;
+  if (b != 16 && b != 32 && b != 64 && b != 128) return false;
   if (n < 3) return false;
   const size_t budget = max_smem > 8192 ? max_smem - 8192 : 0;
   const int maxcols = (int)(budget / ((size_t)2 * b * elem_bytes));
   int seg[kMaxChaseCtas + 1];
-  return maxcols >= 1 && chase_segments(n, b, std::min(kMaxChaseCtas, n), maxcols, seg);
+  if (!(maxcols >= 1 && chase_segments(n, b, std::min(kMaxChaseCtas, n), maxcols, seg))) return false;
+  // The Q2 back-transformation holds one W (2b x b) and T (b x b) block and at least one column of Z per CTA.
+  return (size_t)elem_bytes * ((size_t)n + 3 * (size_t)b * b + 2 * (size_t)b) + 1024 <= max_smem;
 }
 
 size_t q2_tq_elems(int n, int b) { return q2_blocks(n, b).size() * (size_t)b * b + 1; }
@@ -544,7 +549,8 @@ cudaError_t sb2st(int n, int b, const T* ab, T* d, T* e, T* w2, size_t max_smem,
   p.limit_ns = limit_ns;
   if (b == 16) return sb2st_bw<T, 16>(p, max_smem, s);
   if (b == 32) return sb2st_bw<T, 32>(p, max_smem, s);
-  return sb2st_bw<T, 64>(p, max_smem, s);
+  if (b == 64) return sb2st_bw<T, 64>(p, max_smem, s);
+  return sb2st_bw<T, 128>(p, max_smem, s);
 }
 
 template <typename T>
@@ -574,7 +580,8 @@ cudaError_t q2_apply(int n, int b, int m, const T* w2, T* z, int ldz, T* tq, Des
   const int grid = (m + mc - 1) / mc;
   if (b == 16) err = q2_launch<T, 16>(n, b, m, mc, nb, db, w2, tq, z, ldz, grid, smem, tsmem, s);
   else if (b == 32) err = q2_launch<T, 32>(n, b, m, mc, nb, db, w2, tq, z, ldz, grid, smem, tsmem, s);
-  else err = q2_launch<T, 64>(n, b, m, mc, nb, db, w2, tq, z, ldz, grid, smem, tsmem, s);
+  else if (b == 64) err = q2_launch<T, 64>(n, b, m, mc, nb, db, w2, tq, z, ldz, grid, smem, tsmem, s);
+  else err = q2_launch<T, 128>(n, b, m, mc, nb, db, w2, tq, z, ldz, grid, smem, tsmem, s);
   if (err != cudaSuccess) return err;
   return cudaGetLastError();
 }

@@ -631,10 +631,10 @@ __global__ void dc_copy_kernel(DcBufs B, int col_limit) {
   const int mi = blockIdx.x;
   const MergeDesc md = B.merges[mi];
   const MergeInfo inf = B.info[mi];
-  const int s = md.s, n = min(md.n1 + md.n2, col_limit), K = inf.K;
+  const int s = md.s, n = md.n1 + md.n2, ncols = min(n, col_limit), K = inf.K;
   const size_t ld = B.ld;
   // One column per CTA (while the grid allows): enough CTAs in flight to cover the copy's memory latency.
-  for (int c = blockIdx.y; c < n; c += gridDim.y) {
+  for (int c = blockIdx.y; c < ncols; c += gridDim.y) {
     const int src = B.outSrc[s + c];
     const double* from = (src < K ? B.Qa : B.Qc) + (size_t)s + (size_t)(s + src) * ld;
     double* to = B.Qb + (size_t)s + (size_t)(s + c) * ld;

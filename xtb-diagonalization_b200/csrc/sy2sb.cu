@@ -224,16 +224,16 @@ inline int yk_split(int m) { return std::max(1, std::min(kMaxSplit, m / 128)); }
 }  // namespace
 
 bool sy2sb_supported(int n, int b, size_t max_smem, int elem_bytes) {
-  if (b != 16 && b != 32 && b != 64) return false;
+  if (b != 16 && b != 32 && b != 64 && b != 128) return false;
   if (n < 3) return false;
   const int ldp = panel_ldp(n, b);
   size_t need;
   if (elem_bytes == 8) {
     need = b == 16 ? panel_smem_bytes<double, 16>(ldp) : b == 32 ? panel_smem_bytes<double, 32>(ldp)
-                                                                 : panel_smem_bytes<double, 64>(ldp);
+         : b == 64 ? panel_smem_bytes<double, 64>(ldp) : panel_smem_bytes<double, 128>(ldp);
   } else {
     need = b == 16 ? panel_smem_bytes<float, 16>(ldp) : b == 32 ? panel_smem_bytes<float, 32>(ldp)
-                                                                : panel_smem_bytes<float, 64>(ldp);
+         : b == 64 ? panel_smem_bytes<float, 64>(ldp) : panel_smem_bytes<float, 128>(ldp);
   }
   return need + 1024 <= max_smem;
 }
@@ -270,7 +270,10 @@ cudaError_t sy2sb(int n, int b, T* a, int lda, T* v1, T* t1, T* tau1, T* ab, T* 
     pp.tf = t1 + (size_t)p * b * b;
     pp.mr = (m + kPanelCluster - 1) / kPanelCluster;
     pp.ldp = ldp;
-    err = b == 16 ? launch_panel<T, 16>(pp, s) : b == 32 ? launch_panel<T, 32>(pp, s) : launch_panel<T, 64>(pp, s);
+    err = b == 16   ? launch_panel<T, 16>(pp, s)
+          : b == 32 ? launch_panel<T, 32>(pp, s)
+          : b == 64 ? launch_panel<T, 64>(pp, s)
+                    : launch_panel<T, 128>(pp, s);
     if (err != cudaSuccess) return err;
     T* a22 = a + J + (size_t)J * lda;
     T* x = vwv + (size_t)k * m;  // columns [k, 2k) of vwv: X, then W

@@ -18,9 +18,16 @@
 // M or N contiguous as MN-major tiles (four boxes of 32 x 32, 128-byte swizzle with 32-byte atoms, the layout the
 // tensor core needs for MN-major TF32), so no transpose pass is needed.
 //
+// BF16 (passes 11 and 13).  The same pipeline on kind::f16 with BF16 operands: passes 11 is one BF16 product (8-bit
+// mantissas, about 2^-9 per operand), 13 splits every operand as hi = bf16(x), lo = bf16(x - hi) and keeps
+// hi*hi + hi*lo + lo*hi (about 2^-17).  The split pass writes every BF16 operand K-major (transposing the ones stored
+// with M or N contiguous), so a stage is 64 deep in K (128 bytes per row, the same 16 KB tiles) and every tile is a
+// K-major 128-byte-swizzled box of 64 x 128.
+//
 // Triangular modes (gemm.cuh) are applied by the split pass (the masked triangle becomes zero) and used to clip each
 // tile's K range; kCUpper skips output tiles strictly below the diagonal.
 #include <cuda.h>
+#include <cuda_bf16.h>
 
 #include <algorithm>
 #include <mutex>
@@ -87,11 +94,44 @@ __global__ void umma_split_kernel(const __grid_constant__ SplitParams P) {
   }
 }
 
+// BF16 operands, K-major: dst[k + mn * ldk] for op(X) element (mn, k) (A: (m, k); B: (n, k) of op(B)^T).
+struct SplitJob16 {
+  const float* src;
+  __nv_bfloat16* hi;
+  __nv_bfloat16* lo;
+  int lds, K, MN, ldk;
+  int k_contig;  // 1: the stored operand is contiguous along K
+  int keep;      // 0 all, 1 k >= mn, 2 k <= mn
+};
+
+struct Split16Params {
+  SplitJob16 j[2 * kMaxProbs];
+  int njobs;
+  int pieces;
+};
+
+__global__ void umma_split_bf16_kernel(const __grid_constant__ Split16Params P) {
+  const SplitJob16& J = P.j[blockIdx.y];
+  const size_t total = (size_t)J.ldk * J.MN;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(idx % J.ldk), mn = (int)(idx / J.ldk);
+    float x = 0.f;
+    if (k < J.K && (J.keep == 0 || (J.keep == 1 ? k >= mn : k <= mn)))
+      x = J.k_contig ? J.src[k + (size_t)mn * J.lds] : J.src[mn + (size_t)k * J.lds];
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    J.hi[idx] = h;
+    if (P.pieces == 2) J.lo[idx] = __float2bfloat16_rn(x - __bfloat162float(h));
+  }
+}
+
 __device__ __forceinline__ void record_timeout(const UParams& P, int where) {
   set_status(P.st, kStatusBarrierTimeout, 0, where);
 }
 
+template <bool kBf16>
 __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_constant__ UParams P) {
+  constexpr int kBKe = kBf16 ? 64 : kBK;  // K elements per stage (128 bytes per tile row either way)
   extern __shared__ unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kStages];
   __shared__ __align__(8) uint64_t empty_bar[kStages];
@@ -125,8 +165,8 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
   if (pr.mode & kTriALower) kend = min(kend, m0 + kBM);
   if (pr.mode & kTriBUpper) kend = min(kend, n0 + kBN);
   if (pr.mode & kTriBLower) kbeg = max(kbeg, n0);
-  const int kb0 = kbeg / kBK;
-  const int nk = kend > kbeg ? (kend + kBK - 1) / kBK - kb0 : 0;
+  const int kb0 = kbeg / kBKe;
+  const int nk = kend > kbeg ? (kend + kBKe - 1) / kBKe - kb0 : 0;
   const int passes = P.passes;
 
   if (threadIdx.x == 0) {
@@ -160,11 +200,16 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
       }
       if (s_abort) break;
       unsigned char* st = smem + (size_t)s * kStageBytes;
-      const int k0 = (kb0 + i) * kBK;
+      const int k0 = (kb0 + i) * kBKe;
       umma::mbar_arrive_expect_tx(&full_bar[s], bytes);
       for (int h = 0; h < (passes == 3 ? 2 : 1); ++h) {
         unsigned char* sa = st + h * kTileBytes;
         unsigned char* sb = st + (2 + h) * kTileBytes;
+        if (kBf16) {
+          umma::tma_load_2d(sa, &pr.a[h], &full_bar[s], k0, m0);
+          umma::tma_load_2d(sb, &pr.b[h], &full_bar[s], k0, n0);
+          continue;
+        }
         if (pr.a_mn) {
           for (int c = 0; c < kBM / 32; ++c) umma::tma_load_2d(sa + c * 4096, &pr.a[h], &full_bar[s], m0 + 32 * c, k0);
         } else {
@@ -179,7 +224,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
     }
   } else if (nk > 0 && warp == 1 && lane == 0) {
     // MMA issuer.
-    const uint32_t idesc = umma::idesc_tf32(kBM, kBN, pr.a_mn, pr.b_mn);
+    const uint32_t idesc = kBf16 ? umma::idesc_bf16(kBM, kBN) : umma::idesc_tf32(kBM, kBN, pr.a_mn, pr.b_mn);
     for (int i = 0; i < nk; ++i) {
       const int s = i % kStages;
       if (!umma::mbar_wait(&full_bar[s], (i / kStages) & 1, P.limit_ns)) {
@@ -190,19 +235,26 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
       if (s_abort) break;
       umma::tc_fence_after();
       const uint32_t st = umma::smem_addr(smem + (size_t)s * kStageBytes);
+      // Four MMAs per stage: K = 8 (TF32) or 16 (BF16) each, 32 bytes along the 128-byte tile rows.
 #pragma unroll
-      for (int kk = 0; kk < kBK / 8; ++kk) {
+      for (int kk = 0; kk < 4; ++kk) {
         uint64_t ad[2], bd[2];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const uint32_t sa = st + h * kTileBytes, sb = st + (2 + h) * kTileBytes;
-          ad[h] = pr.a_mn ? umma::desc_mnmajor_sw128_32b(sa + kk * 1024, 4096) : umma::desc_kmajor_sw128(sa + kk * 32);
-          bd[h] = pr.b_mn ? umma::desc_mnmajor_sw128_32b(sb + kk * 1024, 4096) : umma::desc_kmajor_sw128(sb + kk * 32);
+          ad[h] = (!kBf16 && pr.a_mn) ? umma::desc_mnmajor_sw128_32b(sa + kk * 1024, 4096)
+                                      : umma::desc_kmajor_sw128(sa + kk * 32);
+          bd[h] = (!kBf16 && pr.b_mn) ? umma::desc_mnmajor_sw128_32b(sb + kk * 1024, 4096)
+                                      : umma::desc_kmajor_sw128(sb + kk * 32);
         }
-        umma::mma_tf32(tmem, ad[0], bd[0], idesc, (i | kk) != 0 ? 1u : 0u);
+        auto mma = [&](uint64_t a, uint64_t b, uint32_t acc) {
+          if (kBf16) umma::mma_bf16(tmem, a, b, idesc, acc);
+          else umma::mma_tf32(tmem, a, b, idesc, acc);
+        };
+        mma(ad[0], bd[0], (i | kk) != 0 ? 1u : 0u);
         if (passes == 3) {
-          umma::mma_tf32(tmem, ad[0], bd[1], idesc, 1u);
-          umma::mma_tf32(tmem, ad[1], bd[0], idesc, 1u);
+          mma(ad[0], bd[1], 1u);
+          mma(ad[1], bd[0], 1u);
         }
       }
       umma::mma_commit(&empty_bar[s]);
@@ -285,7 +337,22 @@ bool encode_operand(CUtensorMap* map, const float* base, int rows, int cols, int
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Tensor map of a K-major BF16 operand (K x MN, leading dimension ldk elements, a multiple of 8): boxes of 64 along K
+// (128 bytes) by 128, 128-byte swizzle.
+bool encode_operand_bf16(CUtensorMap* map, const __nv_bfloat16* base, int K, int MN, int ldk) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)MN};
+  cuuint64_t strides[1] = {(cuuint64_t)ldk * sizeof(__nv_bfloat16)};
+  cuuint32_t box[2] = {64u, 128u};
+  cuuint32_t estr[2] = {1u, 1u};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 inline int pad4(int r) { return (std::max(r, 1) + 3) & ~3; }
+inline int pad8(int r) { return (std::max(r, 1) + 7) & ~7; }
 inline size_t up64(size_t e) { return (e + 63) & ~size_t(63); }
 
 struct OperandShape {
@@ -316,7 +383,7 @@ OperandShape shape_b(const GemmDesc<float>& p) {
 
 size_t operand_elems(const OperandShape& s) { return 2 * up64((size_t)pad4(s.rows) * std::max(s.cols, 1)); }
 
-bool g_smem_set[64];
+bool g_smem_set[2][64];
 
 }  // namespace
 
@@ -331,7 +398,9 @@ size_t umma_work_elems(const GemmDesc<float>* probs, int nprob) {
 
 cudaError_t umma_gemm_group(const GemmDesc<float>* probs, int nprob, int passes, float* work, size_t work_elems,
                             DeviceStatus* st, uint64_t limit_ns, cudaStream_t s) {
-  if (passes != 1 && passes != 3) return cudaErrorInvalidValue;
+  if (passes != 1 && passes != 3 && passes != 11 && passes != 13) return cudaErrorInvalidValue;
+  const bool bf16 = passes > 10;
+  if (bf16) passes -= 10;
   for (int base = 0; base < nprob; base += kMaxProbs) {
     const int cnt = std::min(kMaxProbs, nprob - base);
     if (umma_work_elems(probs + base, cnt) > work_elems) return cudaErrorInvalidValue;
@@ -340,6 +409,9 @@ cudaError_t umma_gemm_group(const GemmDesc<float>* probs, int nprob, int passes,
     SplitParams sp;
     memset(&sp, 0, sizeof(sp));
     sp.passes = passes;
+    Split16Params sp16;
+    memset(&sp16, 0, sizeof(sp16));
+    sp16.pieces = passes == 3 ? 2 : 1;
     float* w = work;
     int tb = 0, used = 0, max_total = 0;
     for (int i = 0; i < cnt; ++i) {
@@ -358,7 +430,38 @@ cudaError_t umma_gemm_group(const GemmDesc<float>* probs, int nprob, int passes,
       q.tiles_n = (p.N + kBN - 1) / kBN;
       q.tile_begin = tb;
       tb += q.tiles_m * q.tiles_n;
-      if (q.K > 0) {
+      if (q.K > 0 && bf16) {
+        q.a_mn = 0;
+        q.b_mn = 0;
+        // op(A) as (m, k) and op(B)^T as (n, k), both K-major.
+        const float* src[2] = {p.A, p.B};
+        const int lds[2] = {p.lda, p.ldb};
+        const int mnd[2] = {p.M, p.N};
+        const int kc[2] = {p.transA ? 1 : 0, p.transB ? 0 : 1};
+        const int keep[2] = {(p.mode & kTriAUpper) ? 1 : (p.mode & kTriALower) ? 2 : 0,
+                             (p.mode & kTriBUpper) ? 2 : (p.mode & kTriBLower) ? 1 : 0};
+        CUtensorMap* maps[2] = {q.a, q.b};
+        for (int o = 0; o < 2; ++o) {
+          const int ldk = pad8(q.K);
+          const size_t half = (size_t)ldk * mnd[o];  // bf16 elements per piece
+          __nv_bfloat16* base = reinterpret_cast<__nv_bfloat16*>(w);
+          SplitJob16& J = sp16.j[sp16.njobs++];
+          J.src = src[o];
+          J.lds = lds[o];
+          J.K = q.K;
+          J.MN = mnd[o];
+          J.ldk = ldk;
+          J.k_contig = kc[o];
+          J.keep = keep[o];
+          J.hi = base;
+          J.lo = base + ((half + 63) & ~size_t(63));
+          w += ((half + 63) & ~size_t(63));  // two BF16 pieces take the room of one FP32 copy
+          max_total = std::max<int>(max_total, (int)std::min<size_t>(half, 1u << 30));
+          if (!encode_operand_bf16(&maps[o][0], J.hi, q.K, mnd[o], ldk) ||
+              !encode_operand_bf16(&maps[o][1], J.lo, q.K, mnd[o], ldk))
+            return cudaErrorInvalidValue;
+        }
+      } else if (q.K > 0) {
         const OperandShape sa = shape_a(p), sb = shape_b(p);
         q.a_mn = sa.mn ? 1 : 0;
         q.b_mn = sb.mn ? 1 : 0;
@@ -398,15 +501,21 @@ cudaError_t umma_gemm_group(const GemmDesc<float>* probs, int nprob, int passes,
       umma_split_kernel<<<dim3(std::max(bx, 1), sp.njobs), 256, 0, s>>>(sp);
       note_launches();
     }
+    if (sp16.njobs > 0) {
+      const int bx = (int)std::min<long>((max_total + 255) / 256, 148 * 4);
+      umma_split_bf16_kernel<<<dim3(std::max(bx, 1), sp16.njobs), 256, 0, s>>>(sp16);
+      note_launches();
+    }
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return err;
-    if (dev < 0 || dev >= 64 || !g_smem_set[dev]) {
-      err = cudaFuncSetAttribute(umma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    auto kern = bf16 ? umma_gemm_kernel<true> : umma_gemm_kernel<false>;
+    if (dev < 0 || dev >= 64 || !g_smem_set[bf16][dev]) {
+      err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
       if (err != cudaSuccess) return err;
-      if (dev >= 0 && dev < 64) g_smem_set[dev] = true;
+      if (dev >= 0 && dev < 64) g_smem_set[bf16][dev] = true;
     }
-    umma_gemm_kernel<<<tb, kThreads, kSmemBytes, s>>>(up);
+    kern<<<tb, kThreads, kSmemBytes, s>>>(up);
     note_launches();
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
