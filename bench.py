@@ -201,6 +201,13 @@ def cpu_chain_time(h, s, budget_s: float, max_runs: int):
     return statistics.median(times), len(times), threads
 
 
+def cpu_reference_solution(h, s):
+    """The reference's LAPACK chain's (w, C) on the same input (the checker of the GPU arm's accuracy fields)."""
+    from oracle import lapack
+
+    return lapack.sygvd_chain(h, s)
+
+
 def cpu_one_thread_time(h, s, runs=3):
     """The same chain with OpenBLAS on one thread (the reference's single-thread protocol): median ms of `runs` after
     one untimed solve; the thread count is restored afterwards."""
@@ -416,7 +423,21 @@ def accuracy_on_device(H, S, lam, C, w, C_ref):
             "s_orthogonality": orth, "density_error_vs_fp64_gpu": float((p - p_ref).abs().max())}
 
 
-def run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush):
+def oracle_errors(dev, W, C, oracle):
+    """Eigenvalue and aufbau-density errors of (W, C) (device) against the CPU LAPACK chain's (w, C)."""
+    import numpy as np
+    import torch
+
+    if oracle is None:
+        return {}
+    w_or, c_or = oracle
+    m = C.shape[0] // 2
+    Co = torch.from_numpy(np.ascontiguousarray(c_or[:, :m])).to(dev)
+    return {"eigenvalue_error_vs_oracle": float((W.cpu() - torch.from_numpy(w_or)).abs().max()),
+            "density_error_vs_oracle": float((2.0 * C[:, :m] @ C[:, :m].T - 2.0 * Co @ Co.T).abs().max())}
+
+
+def run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush, oracle=None):
     """The same n = 1788 solve with precision 32: FP32 congruence, resident sytrd, ormtr and back-transform (FP64
     Cholesky and tridiagonal eigensolve), then FP64 refinement (two Ogita-Aishima steps) on the FP64 pair.  Timed like
     the FP64 path; accuracy against the exact spectrum and the FP64 GPU result."""
@@ -441,6 +462,7 @@ def run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush):
             solve()
         torch.cuda.synchronize(dev)
         acc = accuracy_on_device(H0, S0, lam_t, H.T, W, C64)
+        acc.update(oracle_errors(dev, W, H.T, oracle))
         xtbeig.set_option("stage_timing", 1)
         flush.zero_()
         solve()
@@ -466,9 +488,12 @@ def run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush):
     return out
 
 
-def run_variant_section(args, dev, stream, H0, S0, lam_t, flush, options, steps=3):
+def run_variant_section(args, dev, stream, H0, S0, lam_t, flush, options, steps=3, C64=None, oracle=None):
     """The n = 1788 solve under other library options (e.g. the two-stage reduction): mean ms over `steps` timed
-    solves after 3 warm-ups, stage times of one untimed solve, eigenvalue error against the exact spectrum."""
+    solves after 3 warm-ups, stage times of one untimed solve, eigenvalue error against the exact spectrum; with C64
+    (the FP64 GPU solve's C) the backward error, S-orthogonality and density error (accuracy_on_device), and with
+    `oracle` (the CPU LAPACK chain's (w, C), computed by the cpu_baseline leg) the eigenvalue and density errors
+    against it.  A solve that returns a nonzero info is reported, not raised."""
     import torch
 
     import xtbeig
@@ -485,13 +510,20 @@ def run_variant_section(args, dev, stream, H0, S0, lam_t, flush, options, steps=
         if info != 0:
             raise RuntimeError(f"xtb_dsygvd_device info={info}: {xtbeig.last_error()}")
 
+    acc = {}
     try:
         for k, v in options.items():
             xtbeig.set_option(k, v)
-        for _ in range(3):
-            solve()
+        try:
+            for _ in range(3):
+                solve()
+        except RuntimeError as e:
+            return {"options": options, "failed": str(e)}
         torch.cuda.synchronize(dev)
         err = float((W - lam_t).abs().max())
+        if C64 is not None:
+            acc = accuracy_on_device(H0, S0, lam_t, H.T, W, C64)
+        acc.update(oracle_errors(dev, W, H.T, oracle))
         xtbeig.set_option("stage_timing", 1)
         solve()
         stages = xtbeig.stage_times()
@@ -508,8 +540,10 @@ def run_variant_section(args, dev, stream, H0, S0, lam_t, flush, options, steps=
     finally:
         for k, v in old.items():
             xtbeig.set_option(k, v)
-    return {"options": options, "ms": round(ms, 4), "steps": steps, "warmup": 3, "eigenvalue_error_vs_exact": err,
-            "stages_ms": {k: round(v, 4) for k, v in stages}}
+    out = {"options": options, "ms": round(ms, 4), "steps": steps, "warmup": 3, "eigenvalue_error_vs_exact": err,
+           "stages_ms": {k: round(v, 4) for k, v in stages}}
+    out.update(acc)
+    return out
 
 
 def run_cycle_section(args, dev, stream, H0, S0, lam_t, flush, precision, steps=5):
@@ -896,6 +930,12 @@ def run_ours(args):
     eig_err = float(np.max(np.abs(w - lam)))
     C64 = H.T.contiguous()
     acc64 = accuracy_on_device(H0, S0, lam_t, C64, W.clone(), C64)
+    # The checker for the accuracy fields: the reference's LAPACK chain on the same bytes (the cpu_baseline leg's
+    # computation; one GPU only, never timed here).
+    oracle = None
+    if world == 1 and not args.no_cpu_baseline and not args.hs_bin:
+        oracle = cpu_reference_solution(h_np, s_np)
+        acc64.update(oracle_errors(dev, W, C64, oracle))
 
     # Stage times of one untimed solve (CUDA events at stage boundaries inside the library).
     xtbeig.set_option("stage_timing", 1)
@@ -967,7 +1007,7 @@ def run_ours(args):
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_ms = float(te.item())
 
-    mixed = run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush) if not args.no_mixed else None
+    mixed = run_mixed_section(args, dev, stream, H0, S0, lam_t, C64, flush, oracle) if not args.no_mixed else None
     if mixed:
         mixed["speedup_vs_fp64"] = round(ms_step_max / mixed["ms"], 3)
     cycle = {"fp64": run_cycle_section(args, dev, stream, H0, S0, lam_t, flush, 64)}
@@ -978,12 +1018,19 @@ def run_ours(args):
         cycle["mixed_speedup_vs_fp64"] = round(cycle["fp64"]["ms"] / cycle["mixed"]["ms"], 3)
     two_stage = None
     if not args.no_two_stage:
-        two_stage = {"fp64": run_variant_section(args, dev, stream, H0, S0, lam_t, flush,
-                                                 {"autotune": 0, "reduction": 2, "band_width": 32})}
+        # FP64 at the band widths its panel fits in shared memory; the FP32 chain (then FP64 refinement) with its GEMMs
+        # on each tensor-core engine at b = 32, 64, 128: the accuracy table of the mixed two-stage design.
+        two_stage = {"fp64": {f"b{b}": run_variant_section(args, dev, stream, H0, S0, lam_t, flush,
+                                                           {"autotune": 0, "reduction": 2, "band_width": b},
+                                                           C64=C64, oracle=oracle)
+                              for b in (32, 64)}}
         if not args.no_mixed:
-            two_stage["mixed"] = run_variant_section(args, dev, stream, H0, S0, lam_t, flush,
-                                                     {"autotune": 0, "reduction": 2, "band_width": 32,
-                                                      "precision": 32})
+            engines = {"tf32": 1, "3xtf32": 3, "bf16": 11, "3xbf16": 13}
+            two_stage["mixed"] = {
+                f"{name}_b{b}": run_variant_section(args, dev, stream, H0, S0, lam_t, flush,
+                                                    {"autotune": 0, "reduction": 2, "band_width": b, "precision": 32,
+                                                     "mixed_gemm": eng}, C64=C64, oracle=oracle)
+                for name, eng in engines.items() for b in (32, 64, 128)}
     batch = run_batch_section(args, dev, stream, rank, world) if args.batch_count > 0 else None
     adjoint = run_adjoint_section(args, dev) if args.adjoint_count > 0 else None
 
