@@ -83,9 +83,11 @@ __device__ __forceinline__ bool group_barrier(unsigned* counter, unsigned member
     const unsigned target = epoch * members;
     uint64_t t0 = 0;
     unsigned spins = 0;
+    // One load per poll: the status word (another CTA's failure) is read with the time check, every 64 polls, so a
+    // poll is one round trip instead of two dependent ones.
     while ((int)(ld_acquire_u32(counter) - target) < 0) {
-      if (ld_volatile_i32(&st->code) != 0) { ok = 0; break; }
       if ((++spins & 63u) == 0) {
+        if (ld_volatile_i32(&st->code) != 0) { ok = 0; break; }
         uint64_t t = global_ns();
         if (t0 == 0) t0 = t;
         else if (t - t0 > limit_ns) {

@@ -134,9 +134,11 @@ __global__ void __launch_bounds__(kChaseThreads, 1) sb2st_kernel(const __grid_co
           const unsigned long long want = task_key(ds, dt);
           uint64_t t0 = 0;
           unsigned spins = 0;
+          // Polls read only the peer's shared-memory progress key; the global status word (a failure elsewhere) is
+          // read with the time check every 256 polls.
           while (ld_acquire_cluster_u64(pr) < want) {
-            if (ld_volatile_i32(&p.st->code) != 0) { ok = 0; break; }
             if ((++spins & 255u) == 0) {
+              if (ld_volatile_i32(&p.st->code) != 0) { ok = 0; break; }
               const uint64_t now = global_ns();
               if (t0 == 0) t0 = now;
               else if (now - t0 > p.limit_ns) {

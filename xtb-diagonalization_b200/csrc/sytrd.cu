@@ -223,10 +223,11 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
       const int qrow = q0 + ((lane >> 2) & 7);
       if ((lane & 3) == 0 && qrow < R) red[qrow * NW + warp] = rs;
     }
-    // A(r, k-1) after the update, for the next column: the thread that owns column k-1 (and just wrote it) reads it
-    // back, so the element loop above carries no per-element test for it.
-    if (tid == tk) {
-      for (int q = 0; q < R; ++q) {
+    // A(r, k-1) after the update, for the next column: the warp of the thread that owns column k-1 (and just wrote
+    // it) reads it back, one row per lane, so the element loop above carries no per-element test for it.
+    if (warp == (tk >> 5)) {
+      __syncwarp();
+      for (int q = lane; q < R; q += 32) {
         if (cta + q * G >= k) break;
         colk[q] = rows[q * ldr + (k - 1)];
       }
