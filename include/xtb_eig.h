@@ -145,12 +145,14 @@ int xtb_dgemm_device(int transa, int transb, int m, int n, int k, double alpha, 
  * Sources/Diagonalization/SBROptions.swift:73-82): times candidate plans for generalized solves of size n at the given
  * precision (64 or 32) on a seeded synthetic pair built on the device - the reduction (one stage on all, 3/4 or 1/2 of
  * the SMs; two stages with band width 16, 32 or 64), then ormtr's compact-WY block size, then (precision 32) the FP32
- * GEMM engine, then (n >= 512) the FP64 engine of the large GEMMs, DMMA or int8 Ozaki - and keeps the fastest.  With the option "autotune" = 1, every later solve uses the tuned plan of the
+ * GEMM engine, then (n >= 512) the FP64 engine of the large GEMMs, DMMA or int8 Ozaki, then the divide and conquer's
+ * leaf size - and keeps the fastest.  With the option "autotune" = 1, every later solve uses the tuned plan of the
  * nearest tuned size (log scale) for its precision.  Work is queued on `stream` (NULL: the library's own stream).
  * Returns 0, -1 / -2 for an invalid n / precision, -3 if no candidate completed, or a CUDA/device error code. */
 int xtb_gpu_autotune(int n, int precision, void* stream);
 /* The tuned plan of (n, precision) as text ("reduction=1 band_width=32 sytrd_grid=0 ormtr_nb=128 mixed_gemm=3
- * dgemm=1 ms=15.4321") into buf (len bytes, NUL-terminated); returns the text length, or -1 if that size was not tuned. */
+ * dgemm=1 dc_leaf=32 ms=15.4321") into buf (len bytes, NUL-terminated); returns the text length, or -1 if that size was
+ * not tuned. */
 int xtb_gpu_tuned_plan(int n, int precision, char* buf, int len);
 
 /* A batch of independent generalized problems (host arrays, itype 1, jobz 'V', uplo 'U'): problem i has size n[i],
@@ -205,7 +207,8 @@ int xtb_dsygvd_density_adjoint_batched(int count, const int* n, const double* co
  * FP64 as xtb_dsygvd_refine_device does), "refine_iters" (refinement steps of the mixed path, default 2; 0 keeps the
  * plain FP32 vectors, about 1e-6 accurate), "backtransform" (1, default: generalized one-stage solves with n >= 512
  * form Q and X Q = U^-1 Q beside the tridiagonal eigensolve and finish with one GEMM C = (X Q) Z; 0: ormtr on Z, then
- * X (Q Z)),
+ * X (Q Z)), "dc_leaf" (0, default: the divide and conquer recurses to 1 x 1 leaves; 16, 32 or 64: the subtrees of
+ * at most that size are diagonalised directly, one CTA each, and the merge levels below them are skipped),
  * "mixed_gemm" (engine of the mixed path's FP32 GEMMs: 3 = 3xTF32 on the tcgen05 tensor cores, default; 1 = TF32;
  * 0 = FP32 on the CUDA cores), "reduction" (1 = one-stage resident sytrd, default; 2 = two-stage sy2sb + sb2st),
  * "band_width" (two-stage band width 16, 32 default, 64), "autotune" (1: use xtb_gpu_autotune's plans),

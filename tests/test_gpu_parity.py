@@ -175,3 +175,67 @@ def test_repeatable_bits(xe):
     w1, z1, _ = xe.stedc(*inputs.random_tridiagonal(300, 1))
     w2, z2, _ = xe.stedc(*inputs.random_tridiagonal(300, 1))
     assert np.array_equal(w1, w2) and np.array_equal(z1, z2)
+
+
+@pytest.fixture(params=[16, 32, 64])
+def leaf(xe, request):
+    old = xe.get_option("dc_leaf")
+    xe.set_option("dc_leaf", request.param)
+    yield request.param
+    xe.set_option("dc_leaf", old)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 16, 17, 31, 32, 33, 63, 64, 65, 100, 131, 257, 412, 1204])
+def test_dstedc_leaf_solver_matches_lapack(xe, leaf, n):
+    """Option "dc_leaf": the subtrees of at most 16 / 32 / 64 are diagonalised directly (Jacobi, one CTA each) and
+    the merge levels below them skipped.  Same bars as the 1 x 1 leaves: eigenvalues within 5e-14 n ||T|| of dstedc,
+    residual and orthogonality <= 1e-13 n, ascending order."""
+    d, e = inputs.random_tridiagonal(n, 700 + n)
+    w_ref, _, info_ref = lapack.stedc(d, e)
+    w, z, info = xe.stedc(d, e)
+    assert info == 0 and info_ref == 0
+    t = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+    scale = max(np.abs(d).max(), np.abs(e).max() if n > 1 else 0.0) * max(n, 1)
+    np.testing.assert_allclose(w, w_ref, rtol=0, atol=5e-14 * scale)
+    assert np.all(np.diff(w) >= 0)
+    _, res, orth = metrics.eigen_accuracy(t, w_ref, w, z)
+    assert res < 1e-13 * max(n, 1) and orth < 1e-13 * max(n, 1)
+
+
+@pytest.mark.parametrize("kind", ["zero_offdiag", "diagonal_ties", "split", "glued_wilkinson", "toeplitz"])
+def test_dstedc_leaf_solver_hard_cases(xe, leaf, kind):
+    n = 150
+    rng = np.random.default_rng(19)
+    if kind == "zero_offdiag":
+        d, e = rng.uniform(-1, 1, n), np.zeros(n - 1)
+    elif kind == "diagonal_ties":
+        d, e = np.repeat(np.array([0.5, -0.25, 1.0, 0.0, 0.5]), n // 5), 1e-9 * rng.uniform(-1, 1, n - 1)
+    elif kind == "split":
+        d, e = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n - 1)
+        e[::7] = 0.0
+    elif kind == "glued_wilkinson":
+        blk = np.abs(np.arange(21) - 10).astype(float)
+        d, e = np.resize(blk, n), np.ones(n - 1)
+        e[20::21] = 1e-8
+    else:
+        d, e = np.full(n, 2.0), np.full(n - 1, -1.0)
+    t = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+    w_ref = np.linalg.eigvalsh(t)
+    w, z, info = xe.stedc(d, e)
+    assert info == 0
+    scale = max(np.abs(d).max(), np.abs(e).max(), 1e-300) * n
+    np.testing.assert_allclose(w, w_ref, rtol=0, atol=5e-14 * scale)
+    _, res, orth = metrics.eigen_accuracy(t, w_ref, w, z)
+    assert res < 1e-13 * n and orth < 1e-13 * n
+
+
+@pytest.mark.parametrize("n", [300, 1204])
+def test_sygvd_with_leaf_solver(xe, leaf, n):
+    h, s, lam = inputs.generalized(n, seed=800 + n)
+    w_ref, c_ref = lapack.sygvd_chain(h, s)
+    w, c, u, info = xe.dsygvd(h, s)
+    assert info == 0
+    assert np.max(np.abs(w - lam)) < 1e-10 and np.max(np.abs(w - w_ref)) < 1e-12
+    assert metrics.backward_error(h, s, w, c) < 10
+    assert metrics.s_orthogonality(s, c) < 1e-12
+    assert metrics.density_error(c, c_ref, metrics.aufbau(n, n // 2)) < 1e-9

@@ -57,6 +57,7 @@ std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (
 std::atomic<long> g_autotune{0};      // 1: solves use the autotuned plan nearest their size (xtb_gpu_autotune)
 std::atomic<long> g_batch_grid{1};    // 1: batch workers size each resident reduction's grid to its matrix
 std::atomic<long> g_dgemm_engine{1};  // FP64 GEMMs: 0 DMMA, 1 Ozaki (int8 tcgen05) where eligible, 2 Ozaki always
+std::atomic<long> g_dc_leaf{0};       // divide and conquer: subtrees of at most this size solved directly (0: none)
 std::atomic<long> g_backtransform{1};  // 1: C = (X Q) Z with X Q formed beside the tridiagonal eigensolve (n >= 512)
 std::atomic<long> g_test_stall{0};    // failure-detection test hook: 1 makes the resident reduction's barriers unreachable
 
@@ -72,10 +73,12 @@ struct Plan {
   int dgemm = 0;       // FP64 GEMM engine of the large GEMMs: 0 DMMA, 1 or 2 int8 Ozaki
   int batch_grid = 0;  // 1: a batch worker's solve, its resident reduction sized to its matrix (sytrd_grid 0)
   int xq = 1;          // generalized one-stage solves with n >= kXqMinN: C = (X Q) Z, X Q formed beside the D&C
+  int leaf = 0;        // divide and conquer leaf size (0: 1 x 1 leaves; 16, 32, 64: direct solves of the subtrees)
   double ms = 0.0;     // measured time of the tuned plan
   long long sig() const {
     return (long long)reduction | (long long)band << 4 | (long long)sytrd_grid << 12 | (long long)ormtr_nb << 24 |
-           (long long)mixed_gemm << 36 | (long long)dgemm << 40 | (long long)batch_grid << 42 | (long long)xq << 43;
+           (long long)mixed_gemm << 36 | (long long)dgemm << 40 | (long long)batch_grid << 42 | (long long)xq << 43 |
+           (long long)(leaf / 16) << 44;
   }
 };
 
@@ -94,6 +97,7 @@ Plan options_plan() {
   p.mixed_gemm = (int)g_mixed_gemm.load();
   p.dgemm = (int)g_dgemm_engine.load();
   p.xq = (int)g_backtransform.load();
+  p.leaf = (int)g_dc_leaf.load();
   return p;
 }
 
@@ -581,7 +585,8 @@ void stage_stedc(Call& k, int n, double* d, double* e, double* z, int ldz, int m
   const size_t hb = (size_t)40 * n * sizeof(int) + (size_t)4 * (n + 8) * sizeof(GemmDesc<double>) + 4096;
   char* h = ready ? nullptr : k.template host<char>("stedc.stage", hb);
   if (!k.ok()) return;
-  k.check(stedc_device(n, d, e, z, ldz, w, wb, plan, !ready, h, hb, k.c->d_status, k.s, m_cols), "stedc");
+  k.check(stedc_device(n, d, e, z, ldz, w, wb, plan, !ready, h, hb, k.c->d_status, k.s, m_cols, t_plan.leaf),
+          "stedc");
   if (k.ok()) ready = true;
 }
 
@@ -815,6 +820,7 @@ void stedc_host(const int* n_, T* d, T* e, T* z, const int* ldz_, T* work, const
   if (ldz < n) { *info = -6; return; }
   Context* c = context();
   if (!c) { *info = t_state.last_code; return; }
+  t_plan = plan_for(n, 64);
   Call k(c, nullptr);
   double* dd = k.template dev<double>("io.sd", n);
   double* de = k.template dev<double>("io.se", n);
@@ -1522,6 +1528,16 @@ int xtb_gpu_autotune(int n, int precision, void* stream) {
     p.dgemm = r.dgemm == 1 ? 0 : 1;
     consider(p);
   }
+  {
+    // The divide and conquer's leaf size: 1 x 1 leaves, or direct solves of the subtrees of at most 16 / 32 / 64.
+    const Plan r = best;
+    for (int leaf : {0, 16, 32, 64}) {
+      if (leaf == r.leaf) continue;
+      Plan p = r;
+      p.leaf = leaf;
+      consider(p);
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   t_prec_override = prec0;
@@ -1543,8 +1559,8 @@ int xtb_gpu_tuned_plan(int n, int precision, char* buf, int len) {
   if (it == g_plans.end()) return -1;
   const Plan& p = it->second;
   const int w = std::snprintf(buf, buf && len > 0 ? (size_t)len : 0,
-                              "reduction=%d band_width=%d sytrd_grid=%d ormtr_nb=%d mixed_gemm=%d dgemm=%d ms=%.4f",
-                              p.reduction, p.band, p.sytrd_grid, p.ormtr_nb, p.mixed_gemm, p.dgemm, p.ms);
+                              "reduction=%d band_width=%d sytrd_grid=%d ormtr_nb=%d mixed_gemm=%d dgemm=%d dc_leaf=%d ms=%.4f",
+                              p.reduction, p.band, p.sytrd_grid, p.ormtr_nb, p.mixed_gemm, p.dgemm, p.leaf, p.ms);
   return w;
 }
 
@@ -1696,6 +1712,11 @@ int xtb_gpu_set_option(const char* name, long value) {
     g_backtransform = value;
     return 0;
   }
+  if (!std::strcmp(name, "dc_leaf")) {
+    if (value != 0 && value != 16 && value != 32 && value != 64) return -2;
+    g_dc_leaf = value;
+    return 0;
+  }
   if (!std::strcmp(name, "stage_timing")) { g_stage_timing = value; return 0; }
   if (!std::strcmp(name, "graphs")) { g_graphs = value; return 0; }
   if (!std::strcmp(name, "batch_workers")) { g_batch_workers = value; return 0; }
@@ -1760,6 +1781,7 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "batch_grid")) return g_batch_grid;
   if (!std::strcmp(name, "test_barrier_stall")) return g_test_stall;
   if (!std::strcmp(name, "backtransform")) return g_backtransform;
+  if (!std::strcmp(name, "dc_leaf")) return g_dc_leaf;
   return -1;
 }
 

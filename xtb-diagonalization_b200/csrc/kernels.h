@@ -215,10 +215,11 @@ size_t stedc_work_bytes(int n);
 // once per plan buffer).
 size_t stedc_plan_bytes(int n);
 // m_cols < n: every eigenvalue, but only the eigenvectors of the m_cols smallest (z's first m_cols columns); the top
-// merge forms only those columns.
+// merge forms only those columns.  leaf (0 or 1: none; else at most 64): the subtrees of at most `leaf` are solved
+// directly (Jacobi, one CTA each) instead of by the merge levels below them.
 cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* work, size_t work_bytes, void* plan,
                          bool upload_plan, void* hstage, size_t hstage_bytes, DeviceStatus* st, cudaStream_t s,
-                         int m_cols = 0);
+                         int m_cols = 0, int leaf = 0);
 
 // ---------------------------------------------------------------------------------------------------- potrf / trtri
 // S = U^T U (upper, in place) and X = U^-1 (upper, strict lower part zero) in one recursion; t: n x n scratch (ld n).

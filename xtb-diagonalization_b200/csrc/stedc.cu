@@ -126,6 +126,148 @@ __global__ void dc_identity_kernel(int n, int ld, double* q, double* qb, const d
   }
 }
 
+// ------------------------------------------------------------------------------------------------ leaves
+
+constexpr int kLeafMax = 64;
+
+// Leaf blocks: the subtrees of the tear tree at depth `depth` (every one of them at most kLeafMax long), each solved
+// directly by one CTA instead of by the merge levels below it.  Block i is found by walking the tree's halving from
+// the root along the bits of i (most significant first), the same split as build_levels: [a, b) -> [a, a + (b-a)/2),
+// [a + (b-a)/2, b).  The block's tridiagonal is the scaled one with the tears of its two ends only (its inner splits
+// are not torn because no merge undoes them); cyclic Jacobi with a round-robin ordering (m/2 disjoint rotations per
+// round) diagonalises it in shared memory, and its eigenvalues (ascending) and eigenvectors become the block's entry
+// state of the first merge level: dd / dnext and the diagonal block of both eigenvector buffers.
+__global__ void __launch_bounds__(256) dc_leaf_kernel(int n, int depth, const double* __restrict__ d,
+                                                      const double* __restrict__ ee, const double* __restrict__ scale,
+                                                      double* dd, double* dnext, double* qa, double* qb, int ld) {
+  extern __shared__ __align__(16) unsigned char leaf_smem[];  // a and v, kLeafMax x (kLeafMax + 1) each
+  double(*a)[kLeafMax + 1] = reinterpret_cast<double(*)[kLeafMax + 1]>(leaf_smem);
+  double(*v)[kLeafMax + 1] = a + kLeafMax;
+  __shared__ double red[32];
+  __shared__ double rot_c[kLeafMax / 2], rot_s[kLeafMax / 2];
+  __shared__ int rot_p[kLeafMax / 2], rot_q[kLeafMax / 2];
+  __shared__ int perm[kLeafMax];
+  int lo = 0, hi = n;
+  for (int l = depth - 1; l >= 0; --l) {
+    const int mid = lo + (hi - lo) / 2;
+    if ((blockIdx.x >> l) & 1) lo = mid;
+    else hi = mid;
+  }
+  const int m = hi - lo;
+  if (m <= 0 || m > kLeafMax) return;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const double sc = scale[0];
+  const double inv = sc > 0.0 ? 1.0 / sc : 1.0;
+  for (int t = tid; t < m * m; t += nt) {
+    const int r = t % m, c = t / m;
+    double x = 0.0;
+    if (r == c) {
+      x = d[lo + r] * inv;
+      if (r == 0 && lo > 0) x -= fabs(ee[lo - 1]);
+      if (r == m - 1 && hi < n) x -= fabs(ee[hi - 1]);
+    } else if (r == c + 1 || c == r + 1) {
+      x = ee[lo + min(r, c)];
+    }
+    a[r][c] = x;
+    v[r][c] = r == c ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  const int kp = (m + 1) & ~1;
+  for (int sweep = 0; sweep < 30 && m > 1; ++sweep) {
+    double off = 0.0, dg = 0.0;
+    for (int t = tid; t < m * m; t += nt) {
+      const int r = t % m, c = t / m;
+      if (r != c) off += a[r][c] * a[r][c];
+      else dg += a[r][c] * a[r][c];
+    }
+    off = block_sum(off, red);
+    dg = block_sum(dg, red);
+    if (off <= 1e-32 * dg || off == 0.0) break;
+    for (int round = 0; round < kp - 1; ++round) {
+      if (tid < kp / 2) {
+        auto at = [&](int pos) { return pos == 0 ? 0 : 1 + (round + pos - 1) % (kp - 1); };
+        int p = at(tid), q = at(kp - 1 - tid);
+        if (p > q) { const int x = p; p = q; q = x; }
+        double c = 1.0, sn = 0.0;
+        if (q < m) {
+          const double apq = a[p][q];
+          if (apq != 0.0) {
+            const double tau = (a[q][q] - a[p][p]) / (2.0 * apq);
+            double t;
+            if (fabs(tau) > 1e150) t = 0.5 / tau;
+            else t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+            c = rsqrt(1.0 + t * t);
+            sn = t * c;
+          }
+        }
+        rot_p[tid] = p;
+        rot_q[tid] = q;
+        rot_c[tid] = c;
+        rot_s[tid] = sn;
+      }
+      __syncthreads();
+      for (int t = tid; t < (kp / 2) * m; t += nt) {  // rows p, q of a
+        const int r = t / m, j = t % m;
+        const int p = rot_p[r], q = rot_q[r];
+        if (q >= m) continue;
+        const double c = rot_c[r], sn = rot_s[r];
+        const double xp = a[p][j], xq = a[q][j];
+        a[p][j] = c * xp - sn * xq;
+        a[q][j] = sn * xp + c * xq;
+      }
+      __syncthreads();
+      for (int t = tid; t < (kp / 2) * m; t += nt) {  // columns p, q of a and of v
+        const int r = t / m, i = t % m;
+        const int p = rot_p[r], q = rot_q[r];
+        if (q >= m) continue;
+        const double c = rot_c[r], sn = rot_s[r];
+        double xp = a[i][p], xq = a[i][q];
+        a[i][p] = c * xp - sn * xq;
+        a[i][q] = sn * xp + c * xq;
+        xp = v[i][p];
+        xq = v[i][q];
+        v[i][p] = c * xp - sn * xq;
+        v[i][q] = sn * xp + c * xq;
+      }
+      __syncthreads();
+    }
+  }
+  // ascending order of the eigenvalues (ties by index)
+  if (tid < m) {
+    const double di = a[tid][tid];
+    int r = 0;
+    for (int j = 0; j < m; ++j) {
+      const double dj = a[j][j];
+      r += (okey(dj) < okey(di) || (okey(dj) == okey(di) && j < tid)) ? 1 : 0;
+    }
+    perm[r] = tid;
+  }
+  __syncthreads();
+  if (tid < m) {
+    const double lam = a[perm[tid]][perm[tid]];
+    dd[lo + tid] = lam;
+    dnext[lo + tid] = lam;
+  }
+  for (int t = tid; t < m * m; t += nt) {
+    const int r = t % m, c = t / m;
+    const double x = v[r][perm[c]];
+    qa[(size_t)(lo + r) + (size_t)(lo + c) * ld] = x;
+    qb[(size_t)(lo + r) + (size_t)(lo + c) * ld] = x;
+  }
+}
+
+// Depth of the leaf blocks for leaves of at most `leaf` (0 or 1: the tree goes down to 1 x 1 leaves, no leaf solve):
+// the first depth at which the largest block (the larger half, repeatedly) is at most `leaf`.
+int leaf_depth(int n, int leaf) {
+  if (leaf <= 1) return -1;
+  int d = 0, mx = n;
+  while (mx > leaf) {
+    mx = mx - mx / 2;
+    ++d;
+  }
+  return d;
+}
+
 // Block-wide exclusive scan of one int per thread; returns the exclusive prefix, *total receives the sum.
 __device__ int block_exscan(int v, int* scratch, int* total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -705,9 +847,10 @@ size_t stedc_plan_bytes(int n) {
 
 cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* work, size_t work_bytes, void* plan,
                          bool upload_plan, void* hstage, size_t hstage_bytes, DeviceStatus* st, cudaStream_t s,
-                         int m_cols) {
+                         int m_cols, int leaf) {
   if (n <= 0) return cudaSuccess;
   if (m_cols <= 0 || m_cols > n) m_cols = n;
+  if (leaf > kLeafMax) leaf = kLeafMax;
   if (work_bytes < stedc_work_bytes(n)) return cudaErrorInvalidValue;
   char* p = reinterpret_cast<char*>(work);
   char* pp = reinterpret_cast<char*>(plan);
@@ -823,7 +966,17 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
     const int blocks = (int)std::min<size_t>((nn + 255) / 256, 4096);
     dc_identity_kernel<<<blocks, 256, 0, s>>>(n, n, B.Qa, B.Qb, B.dd, dnext); note_launches();
   }
-  for (int l = 0; l < L; ++l) {
+  // With leaves, the levels at the leaf depth and below are replaced by one direct solve per leaf block.
+  const int D = leaf_depth(n, leaf);
+  int l_first = 0;
+  if (D >= 0) {
+    const size_t lsmem = (size_t)2 * kLeafMax * (kLeafMax + 1) * sizeof(double);
+    err = allow_max_dynamic_smem(dc_leaf_kernel);
+    if (err != cudaSuccess) return err;
+    dc_leaf_kernel<<<1 << D, 256, lsmem, s>>>(n, D, d, B.ee, B.scale, B.dd, dnext, B.Qa, B.Qb, n); note_launches();
+    l_first = std::max(0, L - D);  // levels[l] holds the merges at depth L - 1 - l
+  }
+  for (int l = l_first; l < L; ++l) {
     const int nm = (int)levels[l].merges.size();
     int maxn = 0;
     for (const auto& m : levels[l].merges) maxn = std::max(maxn, m.n1 + m.n2);
