@@ -207,8 +207,9 @@ int xtb_dsygvd_density_adjoint_batched(int count, const int* n, const double* co
  * FP64 as xtb_dsygvd_refine_device does), "refine_iters" (refinement steps of the mixed path, default 2; 0 keeps the
  * plain FP32 vectors, about 1e-6 accurate), "backtransform" (1, default: generalized one-stage solves with n >= 512
  * form Q and X Q = U^-1 Q beside the tridiagonal eigensolve and finish with one GEMM C = (X Q) Z; 0: ormtr on Z, then
- * X (Q Z)), "dc_leaf" (0, default: the divide and conquer recurses to 1 x 1 leaves; 16, 32 or 64: the subtrees of
- * at most that size are diagonalised directly, one CTA each, and the merge levels below them are skipped),
+ * X (Q Z)), "dc_leaf" (16, default, 32 or 64: the divide and conquer's subtrees of at most that size are
+ * diagonalised directly by Jacobi, one CTA each, and the merge levels below them are skipped; 0: it recurses to 1 x 1
+ * leaves),
  * "mixed_gemm" (engine of the mixed path's FP32 GEMMs: 3 = 3xTF32 on the tcgen05 tensor cores, default; 1 = TF32;
  * 0 = FP32 on the CUDA cores), "reduction" (1 = one-stage resident sytrd, default; 2 = two-stage sy2sb + sb2st),
  * "band_width" (two-stage band width 16, 32 default, 64), "autotune" (1: use xtb_gpu_autotune's plans),

@@ -57,7 +57,7 @@ std::atomic<long> g_band_width{32};   // band width of the two-stage reduction (
 std::atomic<long> g_autotune{0};      // 1: solves use the autotuned plan nearest their size (xtb_gpu_autotune)
 std::atomic<long> g_batch_grid{1};    // 1: batch workers size each resident reduction's grid to its matrix
 std::atomic<long> g_dgemm_engine{1};  // FP64 GEMMs: 0 DMMA, 1 Ozaki (int8 tcgen05) where eligible, 2 Ozaki always
-std::atomic<long> g_dc_leaf{0};       // divide and conquer: subtrees of at most this size solved directly (0: none)
+std::atomic<long> g_dc_leaf{16};      // divide and conquer: subtrees of at most this size solved directly (0: none)
 std::atomic<long> g_backtransform{1};  // 1: C = (X Q) Z with X Q formed beside the tridiagonal eigensolve (n >= 512)
 std::atomic<long> g_test_stall{0};    // failure-detection test hook: 1 makes the resident reduction's barriers unreachable
 
@@ -73,7 +73,7 @@ struct Plan {
   int dgemm = 0;       // FP64 GEMM engine of the large GEMMs: 0 DMMA, 1 or 2 int8 Ozaki
   int batch_grid = 0;  // 1: a batch worker's solve, its resident reduction sized to its matrix (sytrd_grid 0)
   int xq = 1;          // generalized one-stage solves with n >= kXqMinN: C = (X Q) Z, X Q formed beside the D&C
-  int leaf = 0;        // divide and conquer leaf size (0: 1 x 1 leaves; 16, 32, 64: direct solves of the subtrees)
+  int leaf = 16;       // divide and conquer leaf size (0: 1 x 1 leaves; 16, 32, 64: direct solves of the subtrees)
   double ms = 0.0;     // measured time of the tuned plan
   long long sig() const {
     return (long long)reduction | (long long)band << 4 | (long long)sytrd_grid << 12 | (long long)ormtr_nb << 24 |

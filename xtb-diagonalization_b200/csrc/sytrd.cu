@@ -8,20 +8,25 @@
 // cooperative kernel keeps the whole symmetric matrix resident: CTA c of G owns rows c, c+G, c+2G, ... (cyclic, so
 // the shrinking trailing matrix stays balanced), in shared memory when they fit (n = 1788 FP64: 13 rows x 1788 x 8 B =
 // 186 KB per CTA on 148 SMs) and otherwise in a global (L2-resident) slab.  Per column k every CTA
-//   1. knows x = A(0:k-1, k) in registers (column c of the trailing matrix lives in thread c mod NT),
-//      computes ||x|| with a block reduction and forms beta, tau, v exactly as every other CTA does (same data,
-//      same reduction order => bit-identical v in all CTAs, no exchange needed);
+//   1. holds x = A(0:k-1, k) in registers (column c of the trailing matrix lives in thread c mod NT) and writes its
+//      warps' partial sums of ||x(0:k-2)||^2 to shared memory (no block-wide sync here);
 //   2. in ONE pass over its own rows applies the previous step's rank-2 update A -= v w^T + w v^T and accumulates
-//      y_r = sum_c A(r,c) v(c) (the update of step k+1 fused with the symv of step k); the per-row partial sums are
-//      combined by a reduce-scatter across the warp's lanes (9 shuffles for 8 rows instead of 40);
-//   3. publishes (y_r, A(r,k-1)) for its rows, meets every CTA at one grid barrier (a release-add on a counter and an
-//      acquire poll, no further fences) and reads every row's pair for its columns.  Two exchange buffers alternate:
-//      a CTA writes buffer p again only two steps later, after the barrier of the step in between, which every CTA
-//      reaches only after it has read buffer p.  (Polling per-value readiness flags instead of one counter was
-//      measured slower: 75k threads polling L2 cost more than one counter round trip.);
+//      (A x)_r with x itself rather than v: v = (scale x(0:k-2), 1), so y = A v = scale (A x)_r + A(r, k-1), and
+//      the Householder scalars are not needed before the pass (the update of step k+1 fused with the symv of step k;
+//      the per-row partial sums are combined by a reduce-scatter across the warp's lanes, 9 shuffles for 8 rows);
+//      the previous w at own rows is formed from the previous y and v at own rows, w = tau y - tau^2/2 (y.v) v, as
+//      the owner of each column forms it;
+//   3. after the pass's __syncthreads (which also publishes the ||x||^2 partials) forms beta, tau, scale and v
+//      exactly as every other CTA does (same data, same summation order => bit-identical v in all CTAs), publishes
+//      (y_r, A(r,k-1)) for its rows, meets every CTA at one grid barrier (a release-add on a counter and an acquire
+//      poll, no further fences) and reads every row's pair for its columns.  Two exchange buffers alternate: a CTA
+//      writes buffer p again only two steps later, after the barrier of the step in between, which every CTA reaches
+//      only after it has read buffer p.  (Polling per-value readiness flags instead of one counter was measured
+//      slower: 75k threads polling L2 cost more than one counter round trip.);
 //   4. forms w = tau y - tau^2/2 (y.v) v and the next x = A(0:k-2, k-1) - v w(k-1) - w v(k-1) redundantly.
-// One grid barrier and three block-level syncs per column; every reduction runs in a fixed order, so results are
-// deterministic and identical across CTAs; every wait is time-limited (device status word, no trap).
+// One grid barrier and two block-level syncs per column; every reduction runs in a fixed order that does not depend
+// on the grid, so results are deterministic, identical across CTAs and the same for every grid size; every wait is
+// time-limited (device status word, no trap).
 #include "common.cuh"
 #include "kernels.h"
 
@@ -101,8 +106,8 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
 
   T* red = reinterpret_cast<T*>(smem_raw);  // [R][NW] per-warp partial row sums
   T* vrow = red + (size_t)R * NW;           // [R] previous v at own rows
-  T* wrow = vrow + R;                       // [R] previous w at own rows
-  T* colk = wrow + R;                       // [R] A(r, k-1) captured by the pass
+  T* yrow = vrow + R;                       // [R] previous y at own rows (with vrow: the previous w at own rows)
+  T* colk = yrow + R;                       // [R] A(r, k-1) captured by the pass
   T* bred = colk + R;                       // [3][NW] block-reduction scratch (rotated)
   T* scal = bred + 3 * NW;                  // [8] broadcast scalars
   T* rows;
@@ -148,51 +153,30 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
   if constexpr (kUpperInPlace) {
     if (!group_barrier(p.counter, members, epoch, p.st, p.limit_ns)) return;
   }
+  // tau and tau^2/2 (y.v) of the previous step: with the previous step's y at own rows (yrow) and v (vrow) they give
+  // its w at own rows, w = tau y - half v, exactly as the owner of each column forms w.
+  T tau_prev = T(0), half_prev = T(0);
   for (int k = n - 1; k >= 1; --k) {
     const int t = n - 1 - k;                   // step index
     T* xch = p.xch + (size_t)(t & 1) * 2 * n;  // (y, column) pairs of this step
     const bool has_prev = (k < n - 1);
-    // ---- 1. Householder vector from x = A(0:k-1, k); alpha = x(k-1).
+    // ---- 1. ||x||^2 of x = A(0:k-2, k) as per-warp partials, summed after the pass's __syncthreads; alpha = x(k-1).
+    //      The pass multiplies by x itself: y = A v = scale A(:, 0:k-2) x + A(:, k-1) with v = (scale x, 1), so the
+    //      Householder scalars are needed only after the pass, off the path in front of it.
     const int tk = (k - 1) % NT, jk = (k - 1) / NT;
     T part = T(0);
+    T xs[CPT];
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
       const int c = tid + j * NT;
-      if (c < k - 1) part += x[j] * x[j];
+      xs[j] = c < k - 1 ? x[j] : T(0);
+      part = fma(xs[j], xs[j], part);
       if (tid == tk && j == jk) scal[0] = x[j];
     }
-    const T xn2 = block_sum_nw<NW>(part, bred);  // its __syncthreads also publishes scal[0], vrow, wrow
-    const T alpha = scal[0];
-    T beta, tau, scale;
-    if (xn2 == T(0)) {
-      beta = alpha; tau = T(0); scale = T(0);
-    } else {
-      // beta = -sign(alpha) ||(alpha, x)||, tau = (beta - alpha)/beta = 1 + |alpha|/||.||: one reciprocal square
-      // root and one division on the column's critical path.
-      const T s2 = alpha * alpha + xn2;
-      const T rn = rsqrt(s2);
-      const T nrm = s2 * rn;
-      beta = alpha >= T(0) ? -nrm : nrm;
-      tau = T(1) + fabs(alpha) * rn;
-      scale = T(1) / (alpha - beta);
-    }
-#pragma unroll
-    for (int j = 0; j < CPT; ++j) {
-      const int c = tid + j * NT;
-      vn[j] = c < k - 1 ? x[j] * scale : (c == k - 1 ? T(1) : T(0));
-    }
-    if (cta == 0 && tid == 0) { p.e[k - 1] = beta; p.tau[k - 1] = tau; }
-    if (cta == k % G) {
-      T* col = p.aout + (size_t)k * p.lda;
-#pragma unroll
-      for (int j = 0; j < CPT; ++j) {
-        const int c = tid + j * NT;
-        if (c < k - 1) col[c] = vn[j];
-        else if (c == k - 1) col[c] = beta;
-      }
-    }
+    part = warp_sum(part);
+    if (lane == 0) bred[warp] = part;
 
-    // ---- 2. fused pass: previous rank-2 update + y = A v over own rows r < k.
+    // ---- 2. fused pass: previous rank-2 update + A x over own rows r < k.
     for (int q0 = 0; q0 < R; q0 += kRowChunk) {
       if (cta + q0 * G >= k) break;
       T acc[kRowChunk];
@@ -203,7 +187,7 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
         const int r = cta + q * G;
         if (q < R && r < k) {
           T* row = rows + q * ldr;
-          const T vr = vrow[q], wr = wrow[q];
+          const T vr = vrow[q], wr = fma(tau_prev, yrow[q], -(half_prev * vr));  // bit for bit the owner's w
 #pragma unroll
           for (int j = 0; j < CPT; ++j) {
             const int c = tid + j * NT;
@@ -214,7 +198,7 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
                 a = fma(-wr, vk[j], a);
                 row[c] = a;
               }
-              acc[qq] = fma(a, vn[j], acc[qq]);
+              acc[qq] = fma(a, xs[j], acc[qq]);
             }
           }
         }
@@ -223,8 +207,8 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
       const int qrow = q0 + ((lane >> 2) & 7);
       if ((lane & 3) == 0 && qrow < R) red[qrow * NW + warp] = rs;
     }
-    // A(r, k-1) after the update, for the next column: the warp of the thread that owns column k-1 (and just wrote
-    // it) reads it back, one row per lane, so the element loop above carries no per-element test for it.
+    // A(r, k-1) after the update, for the next column and for y: the warp of the thread that owns column k-1 (and just
+    // wrote it) reads it back, one row per lane, so the element loop above carries no per-element test for it.
     if (warp == (tk >> 5)) {
       __syncwarp();
       for (int q = lane; q < R; q += 32) {
@@ -232,15 +216,51 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
         colk[q] = rows[q * ldr + (k - 1)];
       }
     }
-    __syncthreads();
-    // ---- 3. publish (y_r, A(r,k-1)) for own rows, then read every row's pair for this thread's columns.
+    __syncthreads();  // publishes red, colk, the ||x||^2 partials and alpha
+    // ---- 3. Householder vector (identical in every CTA: same data, same order).
+    T xn2 = T(0);
+#pragma unroll
+    for (int w = 0; w < NW; ++w) xn2 += bred[w];
+    const T alpha = scal[0];
+    T beta, tau, scale;
+    if (xn2 == T(0)) {
+      beta = alpha; tau = T(0); scale = T(0);
+    } else {
+      // beta = -sign(alpha) ||(alpha, x)||, tau = (beta - alpha)/beta = 1 + |alpha|/||.||: one reciprocal square
+      // root and one division.
+      const T s2 = alpha * alpha + xn2;
+      const T rn = rsqrt(s2);
+      const T nrm = s2 * rn;
+      beta = alpha >= T(0) ? -nrm : nrm;
+      tau = T(1) + fabs(alpha) * rn;
+      scale = T(1) / (alpha - beta);
+    }
+    // ---- 4. publish (y_r, A(r,k-1)) for own rows, y_r = scale (A x)_r + A(r, k-1); keep y_r for the next step's w.
     for (int q = tid; q < R; q += NT) {
       const int r = cta + q * G;
       if (r < k) {
         T y = T(0);
 #pragma unroll
         for (int w = 0; w < NW; ++w) y += red[q * NW + w];
+        y = fma(scale, y, colk[q]);
+        yrow[q] = y;
         st_pair(xch + 2 * (size_t)r, y, colk[q]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) {
+      const int c = tid + j * NT;
+      vn[j] = c < k - 1 ? x[j] * scale : (c == k - 1 ? T(1) : T(0));
+      if (c < k && own_q[j] >= 0) vrow[own_q[j]] = vn[j];
+    }
+    if (cta == 0 && tid == 0) { p.e[k - 1] = beta; p.tau[k - 1] = tau; }
+    if (cta == k % G) {
+      T* col = p.aout + (size_t)k * p.lda;
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        const int c = tid + j * NT;
+        if (c < k - 1) col[c] = vn[j];
+        else if (c == k - 1) col[c] = beta;
       }
     }
     if (!group_barrier(p.counter, members, epoch, p.st, p.limit_ns)) return;
@@ -268,15 +288,13 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
       const int c = tid + j * NT;
-      const T w = tau * yj[j] - half * vn[j];
+      const T w = fma(tau, yj[j], -(half * vn[j]));
       x[j] = c < k - 1 ? colj[j] - vn[j] * wkm1 - w : T(0);
       vk[j] = vn[j];
       wk[j] = w;
-      if (c < k && own_q[j] >= 0) {
-        vrow[own_q[j]] = vn[j];
-        wrow[own_q[j]] = w;
-      }
     }
+    tau_prev = tau;
+    half_prev = half;
   }
 }
 
