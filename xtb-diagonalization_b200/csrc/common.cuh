@@ -111,6 +111,36 @@ __device__ __forceinline__ void group_arrive(unsigned* counter, unsigned& epoch)
   if (threadIdx.x == 0) red_release_add_u32(counter, 1u);
 }
 
+// The waiting half of group_barrier: after group_arrive (and any work that needs no other CTA's data), thread 0 polls
+// until every member has arrived at the CTA's latest epoch, then the CTA syncs (the acquire load and the __syncthreads
+// order the later reads after the other members' released writes).  Same return value and error behaviour as
+// group_barrier.  Must be called by all threads of the CTA.
+__device__ __forceinline__ bool group_wait(unsigned* counter, unsigned members, unsigned epoch, DeviceStatus* st,
+                                           uint64_t limit_ns) {
+  __shared__ int s_wait_ok;
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned target = epoch * members;
+    uint64_t t0 = 0;
+    unsigned spins = 0;
+    while ((int)(ld_acquire_u32(counter) - target) < 0) {
+      if ((++spins & 63u) == 0) {
+        if (ld_volatile_i32(&st->code) != 0) { ok = 0; break; }
+        uint64_t t = global_ns();
+        if (t0 == 0) t0 = t;
+        else if (t - t0 > limit_ns) {
+          set_status(st, kStatusBarrierTimeout, 0, (int)epoch);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    s_wait_ok = ok;
+  }
+  __syncthreads();
+  return s_wait_ok != 0;
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

@@ -16,10 +16,12 @@
 //      the per-row partial sums are combined by a reduce-scatter across the warp's lanes, 9 shuffles for 8 rows);
 //      the previous w at own rows is formed from the previous y and v at own rows, w = tau y - tau^2/2 (y.v) v, as
 //      the owner of each column forms it;
-//   3. after the pass's __syncthreads (which also publishes the ||x||^2 partials) forms beta, tau, scale and v
-//      exactly as every other CTA does (same data, same summation order => bit-identical v in all CTAs), publishes
-//      (y_r, A(r,k-1)) for its rows, meets every CTA at one grid barrier (a release-add on a counter and an acquire
-//      poll, no further fences) and reads every row's pair for its columns.  Two exchange buffers alternate: a CTA
+//   3. after the pass's __syncthreads (which also publishes the ||x||^2 partials) publishes ((A x)_r, A(r,k-1)) for
+//      its rows and arrives at the grid barrier (a release-add on a counter); while the barrier is in flight it forms
+//      beta, tau, scale and v exactly as every other CTA does (same data, same summation order => bit-identical v in
+//      all CTAs), y at its own rows and its output columns; then it waits (an acquire poll, no further fences) and
+//      reads every row's pair for its columns, y = scale (A x) + A(:,k-1) with the owner's fma.  Two exchange buffers
+//      alternate: a CTA
 //      writes buffer p again only two steps later, after the barrier of the step in between, which every CTA reaches
 //      only after it has read buffer p.  (Polling per-value readiness flags instead of one counter was measured
 //      slower: 75k threads polling L2 cost more than one counter round trip.);
@@ -217,7 +219,21 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
       }
     }
     __syncthreads();  // publishes red, colk, the ||x||^2 partials and alpha
-    // ---- 3. Householder vector (identical in every CTA: same data, same order).
+    // ---- 3. publish ((A x)_r, A(r,k-1)) for own rows; (A x)_r is kept in yrow until the scale is known.  The
+    //      consumer forms y_r = scale (A x)_r + A(r, k-1) with the same fma as the owner, so the Householder scalars
+    //      below are computed while the grid barrier is in flight instead of in front of it.
+    for (int q = tid; q < R; q += NT) {
+      const int r = cta + q * G;
+      if (r < k) {
+        T ax = T(0);
+#pragma unroll
+        for (int w = 0; w < NW; ++w) ax += red[q * NW + w];
+        yrow[q] = ax;
+        st_pair(xch + 2 * (size_t)r, ax, colk[q]);
+      }
+    }
+    group_arrive(p.counter, epoch);
+    // ---- 4. Householder vector (identical in every CTA: same data, same order), y at own rows, v.
     T xn2 = T(0);
 #pragma unroll
     for (int w = 0; w < NW; ++w) xn2 += bred[w];
@@ -235,17 +251,8 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
       tau = T(1) + fabs(alpha) * rn;
       scale = T(1) / (alpha - beta);
     }
-    // ---- 4. publish (y_r, A(r,k-1)) for own rows, y_r = scale (A x)_r + A(r, k-1); keep y_r for the next step's w.
     for (int q = tid; q < R; q += NT) {
-      const int r = cta + q * G;
-      if (r < k) {
-        T y = T(0);
-#pragma unroll
-        for (int w = 0; w < NW; ++w) y += red[q * NW + w];
-        y = fma(scale, y, colk[q]);
-        yrow[q] = y;
-        st_pair(xch + 2 * (size_t)r, y, colk[q]);
-      }
+      if (cta + q * G < k) yrow[q] = fma(scale, yrow[q], colk[q]);  // y_r for the next step's w at own rows
     }
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
@@ -263,12 +270,16 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
         else if (c == k - 1) col[c] = beta;
       }
     }
-    if (!group_barrier(p.counter, members, epoch, p.st, p.limit_ns)) return;
+    if (!group_wait(p.counter, members, epoch, p.st, p.limit_ns)) return;
     T yj[CPT], colj[CPT];
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
       yj[j] = colj[j] = T(0);
-      if (tid + j * NT < k) ld_pair(xch + 2 * (size_t)(tid + j * NT), yj[j], colj[j]);
+      if (tid + j * NT < k) {
+        T ax;
+        ld_pair(xch + 2 * (size_t)(tid + j * NT), ax, colj[j]);
+        yj[j] = fma(scale, ax, colj[j]);
+      }
     }
     // y(k-1) and A(k-1,k-1) for w(k-1) and d(k-1), published through the same __syncthreads as y.v.
     T pyv = T(0);
