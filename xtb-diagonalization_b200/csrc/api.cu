@@ -382,12 +382,12 @@ void stage_sytrd(Call& k, int n, const T* dfull, int ldf, T* dout, int lda, T* d
   if (k.ok()) k.check(sytrd_launch<T>(p, pl, k.s), "sytrd launch");
 }
 
-// ormtr's compact-WY block size: the plan's, clamped so that a block's factor ((nb^2 + nb) elements) fits in shared
+// ormtr's compact-WY block size: the plan's, clamped so that a block's factor (nb (nb + 1) + nb elements) fits in shared
 // memory.
 template <typename T>
 int ormtr_block(Call& k) {
   int nbmax = 16;
-  while ((size_t)((nbmax + 16) * (nbmax + 16) + nbmax + 16) * sizeof(T) + 1024 <= k.c->max_smem) nbmax += 16;
+  while ((size_t)((nbmax + 16) * (nbmax + 17) + nbmax + 16) * sizeof(T) + 1024 <= k.c->max_smem) nbmax += 16;
   return std::min(std::max(16, t_plan.ormtr_nb), nbmax);
 }
 

@@ -7,14 +7,16 @@
 // Q = H(n-2) ... H(0), so H(0) is applied first.  Blocks of nb consecutive reflectors are combined into compact WY
 // form once, all blocks in parallel:
 //   V   explicit reflector matrix (n x (n-1)),
-//   G_b = V_b^T V_b                     (grouped GEMM, all blocks in one launch),
-//   T_b forward factor from G_b         (H_j0 ... H_j1 = I - V_b T_b V_b^T; one CTA per block),
+//   G_b = V_b^T V_b                     (split-K grouped GEMM, all blocks and slices in one launch),
+//   T_b forward factor from G_b         (H_j0 ... H_j1 = I - V_b T_b V_b^T; one CTA per block, built by joining
+//                                        diagonal blocks of 16, 32, 64, ...),
 //   Y_b = V_b T_b^T                     (grouped GEMM), since H_j1 ... H_j0 = I - V_b T_b^T V_b^T;
 // then each block is two tensor-core GEMMs on the rows it touches (0 .. j0 + nb - 1):
 //   W = V_b^T Z,   Z -= Y_b W.
 // Larger blocks than the reference's 32 cut the number of passes over Z (n/nb sweeps of an n x m matrix); the extra
 // flops of the explicit Y are n^2 nb per block.
 #include <algorithm>
+#include <vector>
 
 #include "kernels.h"
 #include "wy.cuh"
@@ -69,29 +71,38 @@ cudaError_t ormtr_prepare(int n, const T* a, int lda, const T* tau, int nb, Ormt
     int grid = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
     build_v_kernel<T><<<grid, 256, 0, s>>>(n, a, lda, w.V); note_launches();
   }
-  // Gram matrices of all blocks, one grouped launch.
-  GemmDesc<T>* probs = new GemmDesc<T>[nblocks];
+  // Gram matrices of all blocks as split-K partial products (slices of at least 128 rows, upper triangles only), one
+  // grouped launch, into the Y buffer, which is free until Y is formed; wy_factor_kernel sums the slices in order.
+  int S = kMaxSplit;
+  while (S > 1 && (size_t)nblocks * S * nb * nb > (size_t)n * nm1) --S;
+  std::vector<GemmDesc<T>> probs;
+  probs.reserve((size_t)nblocks * S);
   for (int b = 0; b < nblocks; ++b) {
     const int j0 = b * nb, kb = std::min(nb, nm1 - j0), rows = j0 + kb;
+    const int Sb = gram_slices(rows, S), ks = (rows + Sb - 1) / Sb;
     const T* vb = w.V + (size_t)j0 * n;
-    probs[b] = gemm_problem<T>(kb, kb, rows, T(1), vb, n, 1, vb, n, 0, T(0), w.Tf + (size_t)b * nb * nb, nb);
+    for (int sl = 0; sl < Sb; ++sl) {
+      const int r0 = sl * ks, kr = std::min(ks, rows - r0);
+      probs.push_back(gemm_problem<T>(kb, kb, kr, T(1), vb + r0, n, 1, vb + r0, n, 0, T(0),
+                                      w.Y + ((size_t)b * S + sl) * nb * nb, nb, kCUpper));
+    }
   }
-  cudaError_t err = gemm_run(arena, tc, probs, nblocks, s);
-  if (err != cudaSuccess) { delete[] probs; return err; }
+  cudaError_t err = gemm_run(arena, tc, probs.data(), (int)probs.size(), s);
+  if (err != cudaSuccess) return err;
   {
-    const size_t smem = ((size_t)nb * nb + nb) * sizeof(T);
+    const size_t smem = ((size_t)nb * (nb + 1) + nb) * sizeof(T);
     err = allow_max_dynamic_smem(wy_factor_kernel<T>);
-    if (err != cudaSuccess) { delete[] probs; return err; }
-    wy_factor_kernel<T><<<nblocks, 128, smem, s>>>(nm1, nb, tau, w.Tf); note_launches();
+    if (err != cudaSuccess) return err;
+    wy_factor_kernel<T><<<nblocks, 256, smem, s>>>(nm1, nb, tau, w.Y, S, w.Tf); note_launches();
   }
   // Y_b = V_b T_b^T (op(B) = T_b^T is lower triangular).
+  probs.clear();
   for (int b = 0; b < nblocks; ++b) {
     const int j0 = b * nb, kb = std::min(nb, nm1 - j0), rows = j0 + kb;
-    probs[b] = gemm_problem<T>(rows, kb, kb, T(1), w.V + (size_t)j0 * n, n, 0, w.Tf + (size_t)b * nb * nb, nb, 1,
-                               T(0), w.Y + (size_t)j0 * n, n, kTriBLower);
+    probs.push_back(gemm_problem<T>(rows, kb, kb, T(1), w.V + (size_t)j0 * n, n, 0, w.Tf + (size_t)b * nb * nb, nb,
+                                    1, T(0), w.Y + (size_t)j0 * n, n, kTriBLower));
   }
-  err = gemm_run(arena, tc, probs, nblocks, s);
-  delete[] probs;
+  err = gemm_run(arena, tc, probs.data(), nblocks, s);
   if (err != cudaSuccess) return err;
   return cudaGetLastError();
 }
