@@ -51,7 +51,7 @@ struct DcBufs {
   double* Qb;  // eigenvectors (output of the level)
   double* Qc;  // gathered columns: survivors in GEMM order, then deflated
   double* Up;  // rank-one eigenvectors, rows in GEMM order
-  double* Dl;  // dlamda_i - lambda_j
+  double* rtau;  // root j = dlam[rorg[j]] + rtau[j]; dlam_i - lambda_j is formed as (dlam_i - dlam[rorg[j]]) - rtau[j]
   double* sd;  // sorted d (then updated by deflation)
   double* sz;  // sorted z
   double* dlam;  // survivors' poles
@@ -71,6 +71,7 @@ struct DcBufs {
   int* outSrc;    // output position -> source (j < K: root j; K + t: deflated t)
   int* rotI;
   int* rotJ;
+  int* rorg;      // root j's origin pole (see rtau)
   int* posMerge;  // global position -> merge index at the current level
   MergeDesc* merges;
   MergeInfo* info;
@@ -646,14 +647,15 @@ __global__ void dc_secular_kernel(DcBufs B) {
   double tau;
   const bool ok = secular_root(dl, z, K, inf.rho, j, &o, &tau);
   if (!ok && lane == 0) set_status(B.st, kStatusSecularNoConv, s + j + 1, s);
-  const size_t ld = B.ld;
-  double* col = B.Dl + (size_t)s + (size_t)(s + j) * ld;
-  const double dlo = dl[o];
-  for (int i = lane; i < K; i += 32) col[i] = (dl[i] - dlo) - tau;
-  if (lane == 0) B.lam[s + j] = dlo + tau;
+  if (lane == 0) {
+    B.rorg[s + j] = o;
+    B.rtau[s + j] = tau;
+    B.lam[s + j] = dl[o] + tau;
+  }
 }
 
-// One warp per survivor i: zhat_i^2 = -prod_j (dl_i - lambda_j) / prod_{j != i} (dl_i - dl_j)  (Gu-Eisenstat).
+// One warp per survivor i: zhat_i^2 = -prod_j (dl_i - lambda_j) / prod_{j != i} (dl_i - dl_j)  (Gu-Eisenstat), with
+// dl_i - lambda_j formed from root j's origin pole and offset as (dl_i - dl_o) - tau_j, accurate near the pole.
 __global__ void dc_zhat_kernel(DcBufs B) {
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -665,12 +667,11 @@ __global__ void dc_zhat_kernel(DcBufs B) {
   const MergeInfo inf = B.info[mi];
   const int s = md.s, i = gw - s, K = inf.K;
   if (i >= K) return;
-  const size_t ld = B.ld;
   const double* dl = B.dlam + s;
   const double di = dl[i];
   double prod = 1.0;
   for (int j = lane; j < K; j += 32) {
-    const double del = B.Dl[(size_t)(s + i) + (size_t)(s + j) * ld];
+    const double del = (di - dl[B.rorg[s + j]]) - B.rtau[s + j];
     prod *= (j == i) ? -del : del / (di - dl[j]);
   }
   prod = warp_prod(prod);
@@ -698,15 +699,16 @@ __global__ void dc_vectors_kernel(DcBufs B) {
     if (lane == 0) up[B.slotOf[s]] = 1.0;
     return;
   }
-  const double* dcol = B.Dl + (size_t)s + (size_t)(s + j) * ld;
+  const double* dl = B.dlam + s;
+  const double dlo = dl[B.rorg[s + j]], tau = B.rtau[s + j];
   double ss = 0.0;
   for (int i = lane; i < K; i += 32) {
-    const double u = B.zh[s + i] / dcol[i];
+    const double u = B.zh[s + i] / ((dl[i] - dlo) - tau);
     ss += u * u;
   }
   ss = warp_sum(ss);
   const double inv = 1.0 / sqrt(ss);
-  for (int i = lane; i < K; i += 32) up[B.slotOf[s + i]] = (B.zh[s + i] / dcol[i]) * inv;
+  for (int i = lane; i < K; i += 32) up[B.slotOf[s + i]] = (B.zh[s + i] / ((dl[i] - dlo) - tau)) * inv;
 }
 
 // ------------------------------------------------------------------------------------------------ partial top merge
@@ -827,10 +829,10 @@ size_t stedc_work_bytes(int n) {
   size_t b = 0;
   auto add = [&](size_t bytes) { b += ((bytes + 255) / 256) * 256; };
   add(n * sizeof(double) * 2);         // dd, ee
-  for (int i = 0; i < 5; ++i) add(nn * sizeof(double));  // Qa Qb Qc Up Dl
-  for (int i = 0; i < 10; ++i) add(n * sizeof(double));  // sd sz dlam zk zh lam dval rotc rots dnext
+  for (int i = 0; i < 4; ++i) add(nn * sizeof(double));  // Qa Qb Qc Up
+  for (int i = 0; i < 11; ++i) add(n * sizeof(double));  // rtau sd sz dlam zk zh lam dval rotc rots dnext
   add(sizeof(double) * 4);             // scale
-  for (int i = 0; i < 9; ++i) add(n * sizeof(int));      // sperm typ ndl cand slotOf srcCol outSrc rotI rotJ
+  for (int i = 0; i < 10; ++i) add(n * sizeof(int));     // sperm typ ndl cand slotOf srcCol outSrc rotI rotJ rorg
   // per level: posMerge, merges, info, gemm descriptors (levels <= 32)
   add((size_t)32 * n * sizeof(int));
   add((size_t)32 * (n / 2 + 2) * sizeof(MergeDesc));
@@ -867,7 +869,7 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
   B.Qb = carve<double>(p, nn);
   B.Qc = carve<double>(p, nn);
   B.Up = carve<double>(p, nn);
-  B.Dl = carve<double>(p, nn);
+  B.rtau = carve<double>(p, n);
   B.sd = carve<double>(p, n);
   B.sz = carve<double>(p, n);
   B.dlam = carve<double>(p, n);
@@ -888,6 +890,7 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
   B.outSrc = carve<int>(p, n);
   B.rotI = carve<int>(p, n);
   B.rotJ = carve<int>(p, n);
+  B.rorg = carve<int>(p, n);
   B.info = carve<MergeInfo>(p, (size_t)(n / 2 + 2));
   // The plan (per-level position map, merges, merge-GEMM descriptor skeletons) depends on n only and lives in its
   // own buffer, uploaded once per n: a captured graph never reads host staging that a later call rewrites.
@@ -961,7 +964,7 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
   }
 
   // Index arrays start at 0: an entry that a ranking on non-finite input might leave unwritten stays in range.
-  err = cudaMemsetAsync(B.sperm, 0, (size_t)((char*)(B.rotJ + n) - (char*)B.sperm), s);
+  err = cudaMemsetAsync(B.sperm, 0, (size_t)((char*)(B.rorg + n) - (char*)B.sperm), s);
   if (err != cudaSuccess) return err;
   dc_scale_kernel<<<1, 1024, 0, s>>>(n, d, e, B.scale); note_launches();
   dc_init_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, d, e, B.dd, B.ee, B.scale); note_launches();
