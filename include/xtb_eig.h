@@ -209,7 +209,9 @@ int xtb_dsygvd_density_adjoint_batched(int count, const int* n, const double* co
  * form Q and X Q = U^-1 Q beside the tridiagonal eigensolve and finish with one GEMM C = (X Q) Z; 0: ormtr on Z, then
  * X (Q Z)), "dc_leaf" (16, default, 32 or 64: the divide and conquer's subtrees of at most that size are
  * diagonalised directly by Jacobi, one CTA each, and the merge levels below them are skipped; 0: it recurses to 1 x 1
- * leaves),
+ * leaves), "sytrd_tail" (64, default: the one-stage reduction's last columns, a trailing block of at most that order,
+ * and every column of a matrix of at most that order, are reduced on one CTA in shared memory without grid
+ * barriers; 16 to 128 in steps of 16; 0: the grid kernel reduces every column),
  * "mixed_gemm" (engine of the mixed path's FP32 GEMMs: 3 = 3xTF32 on the tcgen05 tensor cores, default; 1 = TF32;
  * 0 = FP32 on the CUDA cores), "reduction" (1 = one-stage resident sytrd, default; 2 = two-stage sy2sb + sb2st),
  * "band_width" (two-stage band width 16, 32 default, 64), "autotune" (1: use xtb_gpu_autotune's plans),

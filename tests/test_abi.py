@@ -73,3 +73,17 @@ def test_wait_limit_and_test_hook_option_ranges_without_gpu():
     assert xtbeig.get_option("test_barrier_stall") == 0
     with pytest.raises(ValueError):
         xtbeig.set_option("test_barrier_stall", 2)
+
+
+def test_sytrd_tail_option_range_without_gpu():
+    """Option "sytrd_tail": the order of the trailing block finished on one CTA, 0 (off) to 128 in steps of 16."""
+    old = xtbeig.get_option("sytrd_tail")
+    try:
+        for good in (0, 16, 64, 128):
+            xtbeig.set_option("sytrd_tail", good)
+            assert xtbeig.get_option("sytrd_tail") == good
+        for bad in (-16, 50, 144):
+            with pytest.raises(ValueError):
+                xtbeig.set_option("sytrd_tail", bad)
+    finally:
+        xtbeig.set_option("sytrd_tail", old)

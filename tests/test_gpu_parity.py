@@ -239,3 +239,39 @@ def test_sygvd_with_leaf_solver(xe, leaf, n):
     assert metrics.backward_error(h, s, w, c) < 10
     assert metrics.s_orthogonality(s, c) < 1e-12
     assert metrics.density_error(c, c_ref, metrics.aufbau(n, n // 2)) < 1e-9
+
+
+@pytest.mark.parametrize("tail", [128, 64, 0])
+@pytest.mark.parametrize("n", [2, 64, 65, 127, 128, 129, 300, 700])
+def test_dsytrd_tail_stage(xe, tail, n):
+    """Option "sytrd_tail" (default 64): the resident reduction's last columns (every column of a matrix of at most
+    that order) run on one CTA in shared memory; the grid kernel hands the trailing block over.  Both sides of the
+    hand-over size match LAPACK dsytrd with the sytrd bars; 0 keeps the grid kernel throughout."""
+    old = xe.get_option("sytrd_tail")
+    xe.set_option("sytrd_tail", tail)
+    try:
+        a = _sym(n, 700 + n)
+        ar_ref, d_ref, e_ref, tau_ref = lapack.sytrd_upper(a)
+        ar, d, e, tau = xe.sytrd_upper(a)
+    finally:
+        xe.set_option("sytrd_tail", old)
+    scale = np.abs(a).max() * n
+    np.testing.assert_allclose(d, d_ref, rtol=0, atol=1e-11 * scale)
+    np.testing.assert_allclose(e, e_ref, rtol=0, atol=1e-11 * scale)
+    np.testing.assert_allclose(tau, tau_ref, rtol=0, atol=1e-11 * n)
+    np.testing.assert_allclose(np.triu(ar), np.triu(ar_ref), rtol=0, atol=1e-10 * n)
+    assert np.array_equal(np.tril(ar, -1), np.tril(a, -1))
+    w = lapack.stedc(d, e)[0]
+    np.testing.assert_allclose(w, np.linalg.eigvalsh(a), rtol=0, atol=5e-14 * scale)
+
+
+@pytest.mark.parametrize("n", [100, 128, 129, 500])
+def test_ssytrd_tail_stage(xe, n):
+    a = _sym(n, 750 + n).astype(np.float32)
+    _, d_ref, e_ref, _ = lapack.sytrd_upper(a, np.float32)
+    ar, d, e, tau = xe.sytrd_upper(a, np.float32)
+    scale = float(np.abs(a).max()) * n
+    np.testing.assert_allclose(d, d_ref, rtol=0, atol=2e-5 * scale)
+    np.testing.assert_allclose(e, e_ref, rtol=0, atol=2e-5 * scale)
+    w = lapack.stedc(d.astype(np.float64), e.astype(np.float64))[0]
+    np.testing.assert_allclose(w, np.linalg.eigvalsh(a.astype(np.float64)), rtol=0, atol=2e-5 * scale)

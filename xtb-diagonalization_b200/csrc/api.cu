@@ -59,6 +59,7 @@ std::atomic<long> g_batch_grid{1};    // 1: batch workers size each resident red
 std::atomic<long> g_dgemm_engine{1};  // FP64 GEMMs: 0 DMMA, 1 Ozaki (int8 tcgen05) where eligible, 2 Ozaki always
 std::atomic<long> g_dc_leaf{16};      // divide and conquer: subtrees of at most this size solved directly (0: none)
 std::atomic<long> g_backtransform{1};  // 1: C = (X Q) Z with X Q formed beside the tridiagonal eigensolve (n >= 512)
+std::atomic<long> g_sytrd_tail{64};  // the resident reduction's last columns (at most this many) on one CTA (0: off)
 std::atomic<long> g_test_stall{0};    // failure-detection test hook: 1 makes the resident reduction's barriers unreachable
 
 // The tunable choices of one solve.  A solve resolves its plan once (options, or the autotuned table) and every stage
@@ -74,11 +75,12 @@ struct Plan {
   int batch_grid = 0;  // 1: a batch worker's solve, its resident reduction sized to its matrix (sytrd_grid 0)
   int xq = 1;          // generalized one-stage solves with n >= kXqMinN: C = (X Q) Z, X Q formed beside the D&C
   int leaf = 16;       // divide and conquer leaf size (0: 1 x 1 leaves; 16, 32, 64: direct solves of the subtrees)
+  int tail = 64;       // the reduction's trailing block of at most this order finished on one CTA (0: none)
   double ms = 0.0;     // measured time of the tuned plan
   long long sig() const {
     return (long long)reduction | (long long)band << 4 | (long long)sytrd_grid << 12 | (long long)ormtr_nb << 24 |
            (long long)mixed_gemm << 36 | (long long)dgemm << 40 | (long long)batch_grid << 42 | (long long)xq << 43 |
-           (long long)(leaf / 16) << 44;
+           (long long)(leaf / 16) << 44 | (long long)(tail / 16) << 48;
   }
 };
 
@@ -98,6 +100,7 @@ Plan options_plan() {
   p.dgemm = (int)g_dgemm_engine.load();
   p.xq = (int)g_backtransform.load();
   p.leaf = (int)g_dc_leaf.load();
+  p.tail = (int)g_sytrd_tail.load();
   return p;
 }
 
@@ -378,8 +381,29 @@ void stage_sytrd(Call& k, int n, const T* dfull, int ldf, T* dout, int lda, T* d
     p.grows = k.template dev<T>("sytrd.rows", (size_t)pl.grid * pl.rows_per_cta * pl.ldr);
     if (!k.ok()) return;
   }
+  // The last columns (all of them for a small matrix) on one CTA: the grid kernel hands the trailing block over.
+  // The failure-detection hook needs the grid barriers, so it keeps the grid kernel throughout.
+  const int tail = p.extra_members ? 0 : std::min(n, t_plan.tail);
+  if (tail > 1 && tail == n) {
+    k.check(sytrd_tail_launch<T>(p, 0, k.s), "sytrd tail launch");
+    return;
+  }
+  if (tail > 1) {
+    p.k_stop = tail - 1;
+    p.hand = k.template dev<T>("sytrd.hand", (size_t)tail * tail);
+    p.ldh = tail;
+    if (!k.ok()) return;
+  }
   k.check(cudaMemsetAsync(ctr, 0, 64 * sizeof(unsigned), k.s), "sytrd counter");
   if (k.ok()) k.check(sytrd_launch<T>(p, pl, k.s), "sytrd launch");
+  if (k.ok() && tail > 1) {
+    SytrdParams<T> q = p;
+    q.n = tail;
+    q.afull = p.hand;
+    q.ldf = p.ldh;
+    q.k_stop = 0;
+    k.check(sytrd_tail_launch<T>(q, 1, k.s), "sytrd tail launch");
+  }
 }
 
 // ormtr's compact-WY block size: the plan's, clamped so that a block's factor (nb (nb + 1) + nb elements) fits in shared
@@ -1717,6 +1741,11 @@ int xtb_gpu_set_option(const char* name, long value) {
     g_dc_leaf = value;
     return 0;
   }
+  if (!std::strcmp(name, "sytrd_tail")) {
+    if (value < 0 || value > 128 || value % 16 != 0) return -2;
+    g_sytrd_tail = value;
+    return 0;
+  }
   if (!std::strcmp(name, "stage_timing")) { g_stage_timing = value; return 0; }
   if (!std::strcmp(name, "graphs")) { g_graphs = value; return 0; }
   if (!std::strcmp(name, "batch_workers")) { g_batch_workers = value; return 0; }
@@ -1782,6 +1811,7 @@ long xtb_gpu_get_option(const char* name) {
   if (!std::strcmp(name, "test_barrier_stall")) return g_test_stall;
   if (!std::strcmp(name, "backtransform")) return g_backtransform;
   if (!std::strcmp(name, "dc_leaf")) return g_dc_leaf;
+  if (!std::strcmp(name, "sytrd_tail")) return g_sytrd_tail;
   return -1;
 }
 

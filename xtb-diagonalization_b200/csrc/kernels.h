@@ -37,6 +37,11 @@ struct SytrdParams {
   // test hook (option "test_barrier_stall") sets 1, so that no barrier can complete and every wait runs into its
   // time limit and returns an error status instead of hanging.
   int extra_members;
+  // Grid kernel: k_stop > 0 hands the trailing (k_stop + 1) x (k_stop + 1) block over after step k_stop + 1 (that
+  // step's update applied, full symmetric rows into hand, ld ldh) and returns; sytrd_tail_launch finishes it.
+  int k_stop;
+  T* hand;
+  int ldh;
 };
 
 struct SytrdPlan {
@@ -49,6 +54,13 @@ template <typename T>
 SytrdPlan sytrd_plan(int n, int num_sms, size_t max_smem, int grid_override);
 template <typename T>
 cudaError_t sytrd_launch(const SytrdParams<T>& p, const SytrdPlan& pl, cudaStream_t s);
+// The last columns of the reduction on one CTA: the leading m x m block (m = p.n), full symmetric rows in p.afull
+// (ld p.ldf; the whole matrix, or a grid launch's hand-over), reduced in shared memory with block-level syncs only.
+// Writes d(0:m-1) (d(m-1) only when skip_dinit is 0), e, tau and the reflector columns 1..m-1 of p.aout.
+template <typename T>
+size_t sytrd_tail_smem(int m);
+template <typename T>
+cudaError_t sytrd_tail_launch(const SytrdParams<T>& p, int skip_dinit, cudaStream_t s);
 // Variant reading the upper triangle of p.afull == p.aout in place (FP64, rows in shared memory, n <= 2048).
 cudaError_t sytrd_launch_upper_inplace(const SytrdParams<double>& p, const SytrdPlan& pl, cudaStream_t s);
 

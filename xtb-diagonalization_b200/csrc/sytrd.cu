@@ -158,7 +158,8 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
   // tau and tau^2/2 (y.v) of the previous step: with the previous step's y at own rows (yrow) and v (vrow) they give
   // its w at own rows, w = tau y - half v, exactly as the owner of each column forms w.
   T tau_prev = T(0), half_prev = T(0);
-  for (int k = n - 1; k >= 1; --k) {
+  const int k_end = p.k_stop > 0 ? p.k_stop + 1 : 1;  // last step this kernel runs
+  for (int k = n - 1; k >= k_end; --k) {
     const int t = n - 1 - k;                   // step index
     T* xch = p.xch + (size_t)(t & 1) * 2 * n;  // (y, column) pairs of this step
     const bool has_prev = (k < n - 1);
@@ -307,6 +308,126 @@ __global__ void __launch_bounds__(NT, 1) sytrd_resident_kernel(SytrdParams<T> p)
     tau_prev = tau;
     half_prev = half;
   }
+  // Hand-over: the pending update of step k_stop + 1 applied to the trailing block, whose full symmetric rows go to
+  // `hand` (row r of the block is its column r).  vrow, yrow and the scalars are this CTA's own; vk and wk were
+  // formed after the last barrier, so every row of the block is complete.
+  if (p.k_stop > 0 && k_end <= n - 1) {
+    const int m = p.k_stop + 1;
+    for (int q = 0; q < R; ++q) {
+      const int r = cta + q * G;
+      if (r >= m) break;
+      const T* row = rows + q * ldr;
+      const T vr = vrow[q], wr = fma(tau_prev, yrow[q], -(half_prev * vr));
+      T* dst = p.hand + (size_t)r * p.ldh;
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        const int c = tid + j * NT;
+        if (c < m) dst[c] = fma(-wr, vk[j], fma(-vr, wk[j], row[c]));
+      }
+    }
+  }
+}
+
+// The last columns on one CTA.  The trailing block's upper triangle lives in shared memory with an odd leading
+// dimension (row- and column-strided reads spread over the banks) and is updated symmetrically; per column k:
+//   1. every warp sums ||x||^2 of x = A(0:k-2, k) itself (the same lanes and shuffle tree in every warp, so all warps
+//      hold the same value without a block sync), every thread forms beta, tau and scale as the grid kernel does, and
+//      threads c < k write v(c) and the output column;
+//   2. y = A v with four threads per row (row r read along the row for c >= r and down the column for c < r);
+//   3. every warp sums y.v itself; threads r < k form w = tau y - tau^2/2 (y.v) v;
+//   4. the rank-2 update A -= v w^T + w v^T of the upper triangle, eight threads per pair of rows (r, k-1-r).
+// Four block syncs per column and no grid barrier: where the trailing matrix is small the grid kernel's per-column
+// exchange costs more than the work.  Sums run in a fixed order, so results are deterministic.
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, 1) sytrd_tail_kernel(SytrdParams<T> p, int skip_dinit) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int m = p.n, ld = (m & 1) ? m + 2 : m + 1;
+  T* A = reinterpret_cast<T*>(smem_raw);  // upper triangle, A[r * ld + c] for r <= c
+  T* v = A + (size_t)m * ld;
+  T* y = v + m;
+  T* w = y + m;
+  const int tid = threadIdx.x, lane = tid & 31;
+  if (ld_volatile_i32(&p.st->code) != 0) return;  // an earlier stage failed
+  for (int idx = tid; idx < m * m; idx += NT) {
+    const int r = idx / m, c = idx - r * m;
+    if (r <= c) A[r * ld + c] = p.afull[(size_t)r * p.ldf + c];
+  }
+  if (!skip_dinit && tid == 0 && m >= 1) {
+    const T dn = p.afull[(size_t)(m - 1) * p.ldf + (m - 1)];
+    p.d[m - 1] = dn;
+    p.aout[(size_t)(m - 1) + (size_t)(m - 1) * p.lda] = dn;
+  }
+  __syncthreads();
+  const int sub4 = tid & 3;
+  const unsigned qmask = 0xFu << (lane & ~3);
+  for (int k = m - 1; k >= 1; --k) {
+    // 1. Householder vector.
+    T part = T(0);
+    for (int c = lane; c < k - 1; c += 32) part = fma(A[c * ld + k], A[c * ld + k], part);
+    const T xn2 = warp_sum(part);
+    const T alpha = A[(k - 1) * ld + k];
+    T beta, tau, scale;
+    if (xn2 == T(0)) {
+      beta = alpha; tau = T(0); scale = T(0);
+    } else {
+      const T s2 = alpha * alpha + xn2;
+      const T rn = rsqrt(s2);
+      const T nrm = s2 * rn;
+      beta = alpha >= T(0) ? -nrm : nrm;
+      tau = T(1) + fabs(alpha) * rn;
+      scale = T(1) / (alpha - beta);
+    }
+    for (int c = tid; c < k; c += NT) {
+      const T vc = c < k - 1 ? A[c * ld + k] * scale : T(1);
+      v[c] = vc;
+      p.aout[(size_t)c + (size_t)k * p.lda] = c < k - 1 ? vc : beta;
+    }
+    if (tid == 0) { p.e[k - 1] = beta; p.tau[k - 1] = tau; }
+    __syncthreads();
+    // 2. y = A v.
+    for (int r = tid >> 2; r < k; r += NT / 4) {
+      T a0 = T(0), a1 = T(0);
+      int c = sub4;
+      for (; c < r; c += 4) a0 = fma(A[c * ld + r], v[c], a0);
+      for (; c < k; c += 4) a1 = fma(A[r * ld + c], v[c], a1);
+      T sum = a0 + a1;
+      sum += __shfl_xor_sync(qmask, sum, 1);
+      sum += __shfl_xor_sync(qmask, sum, 2);
+      if (sub4 == 0) y[r] = sum;
+    }
+    __syncthreads();
+    // 3. y.v and w; d(k-1) = A(k-1,k-1) - 2 w(k-1) (v(k-1) = 1).
+    T pv = T(0);
+    for (int r = lane; r < k; r += 32) pv = fma(y[r], v[r], pv);
+    const T yv = warp_sum(pv);
+    const T half = T(0.5) * tau * tau * yv;
+    for (int r = tid; r < k; r += NT) w[r] = fma(tau, y[r], -(half * v[r]));
+    if (tid == 0) {
+      const T wkm1 = tau * y[k - 1] - half;
+      const T dk = A[(k - 1) * ld + (k - 1)] - T(2) * wkm1;
+      p.d[k - 1] = dk;
+      p.aout[(size_t)(k - 1) + (size_t)(k - 1) * p.lda] = dk;
+    }
+    __syncthreads();
+    // 4. Rank-2 update of the upper triangle of A(0:k-1, 0:k-1): group g of eight threads takes rows g and k-1-g.
+    {
+      const int g = tid >> 3, sub8 = tid & 7;
+      for (int gg = g; 2 * gg < k; gg += NT / 8) {
+        for (int h = 0; h < 2; ++h) {
+          const int r = h == 0 ? gg : k - 1 - gg;
+          if (h == 1 && r == gg) break;
+          const T vr = v[r], wr = w[r];
+          for (int c = r + sub8; c < k; c += 8) {
+            T a = A[r * ld + c];
+            a = fma(-vr, w[c], a);
+            a = fma(-wr, v[c], a);
+            A[r * ld + c] = a;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
 }
 
 template <typename T, int NT, int CPT>
@@ -396,6 +517,27 @@ cudaError_t sytrd_launch(const SytrdParams<T>& p, const SytrdPlan& pl, cudaStrea
   return cudaErrorInvalidValue;
 }
 
+template <typename T>
+size_t sytrd_tail_smem(int m) {
+  const int ld = (m & 1) ? m + 2 : m + 1;
+  return ((size_t)m * ld + 3 * (size_t)m) * sizeof(T);
+}
+
+template <typename T>
+cudaError_t sytrd_tail_launch(const SytrdParams<T>& p, int skip_dinit, cudaStream_t s) {
+  if (p.n <= 0) return cudaSuccess;
+  auto kern = sytrd_tail_kernel<T, 512>;
+  cudaError_t err = allow_max_dynamic_smem(kern);
+  if (err != cudaSuccess) return err;
+  kern<<<1, 512, sytrd_tail_smem<T>(p.n), s>>>(p, skip_dinit);
+  note_launches();
+  return cudaGetLastError();
+}
+
+template size_t sytrd_tail_smem<double>(int);
+template size_t sytrd_tail_smem<float>(int);
+template cudaError_t sytrd_tail_launch<double>(const SytrdParams<double>&, int, cudaStream_t);
+template cudaError_t sytrd_tail_launch<float>(const SytrdParams<float>&, int, cudaStream_t);
 template SytrdPlan sytrd_plan<double>(int, int, size_t, int);
 template SytrdPlan sytrd_plan<float>(int, int, size_t, int);
 template cudaError_t sytrd_launch<double>(const SytrdParams<double>&, const SytrdPlan&, cudaStream_t);
