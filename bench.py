@@ -9,8 +9,8 @@ Synthetic seeded inputs stand in for the GFN2 H/S dumps the reference reads (non
 
 ours (default):  one step = restore H, S on the device (D2D copy of pristine inputs) + one device-pointer solve on
     torch's current stream, timed with CUDA events per step; L2 is flushed (256 MB write) before every timed step,
-    outside the events.  `value` = mean ms per solve (whole job: summed over replicas for N > 1, see DESIGN.md:
-    single solves do not shard, ranks are independent replicas).  `e2e` = the same solve through the C ABI with
+    outside the events.  `value` = mean ms per solve (whole job: summed over replicas for N > 1, because a single
+    solve does not shard and the ranks are independent replicas).  `e2e` = the same solve through the C ABI with
     pinned HOST buffers (H2D of H and S, D2H of C, U and e inside the timed region).  `roofline` = the resident
     reduction kernel (sytrd): algorithmic bytes 4 n^3 / 3 (its symv reads n^3/6 FP64 elements) / its event-timed
     duration, against the measured HBM copy bandwidth.  `cpu_baseline` = the reference's LAPACK chain (dpotrf, dsygst,

@@ -1,8 +1,9 @@
 """The reference's LAPACK call chain on the CPU, through ctypes (TEST INFRASTRUCTURE ONLY: the oracle).
 
 The reference's eigensolve is LAPACK's: xTB's SCC cycle calls potrf once per geometry, then per cycle dsygst (or the
-congruence H' = X^T H X), dsytrd, dstedc, dormtr and dtrsm (SURVEY call stack A; Sources/Diagonalization/Exports.swift
-:6-115 replaces sytrd/stedc/ormtr with Swift ports of the same LAPACK semantics; CLAPACK.h:9-105 lists the routines).
+congruence H' = X^T H X), dsytrd, dstedc, dormtr and dtrsm (xTB's eigensolve call stack;
+Sources/Diagonalization/Exports.swift:6-115 replaces sytrd/stedc/ormtr with Swift ports of the same LAPACK semantics;
+CLAPACK.h:9-105 lists the routines).
 The reference's own Swift/Accelerate code cannot be built here (no Swift toolchain, Accelerate is macOS only, the xtb
 submodule holding sytrd.c is empty).  This module therefore binds the identical LAPACK routines from OpenBLAS 0.3.30,
 the copy that ships with scipy 1.18.1 (exported as ``scipy_<name>_``; Fortran calling convention: every argument by
@@ -198,7 +199,7 @@ def sygvd(h, s):
 
 
 # --------------------------------------------------------------------------------------------------------------------
-# The full chains, stage by stage, as the reference's SCC eigensolve runs them (SURVEY call stack A).
+# The full chains, stage by stage, as the reference's SCC eigensolve runs them (potrf, sygst, sytrd, stedc, ormtr, trsm).
 
 def syevd_chain(a):
     """Standard problem: dsytrd -> dstedc -> dormtr (config: n=412, all eigenpairs)."""
