@@ -47,8 +47,8 @@ constexpr size_t kSmemBytes = (tile::smem_elems<double>() + kLeafElems) * sizeof
 // not > 0, after recording kStatusNotSPD with the global column (1-based).  The block is the kernel's critical path,
 // so it is factored by 8-column panels (three barriers per panel instead of two per column): the panel's 8 x 8
 // diagonal block by one warp with shuffles, its block row by a triangular solve per column, then the rank-8 update
-// of the trailing triangle with 8-deep dot products.  X is formed by back substitution with one thread per column
-// and 8-row panels (8 independent sums per panel), which needs no barrier.  The frame beyond nb is the identity.
+// of the trailing triangle with 8-deep dot products.  X is formed by blocks: the 8 x 8 diagonal blocks' inverses,
+// then joins of neighbouring blocks of 8, 16, 32.  The frame beyond nb is the identity.
 // With a panel (the kp x nb block row U(j0 - kp : j0, j0 : j0 + nb), ld lda), the block's trailing update
 // A -= P^T P runs first, in shared memory with 8 x 4 register tiles per thread (gsm: the tile pipeline's region,
 // free while the leaf runs, holds P).
@@ -208,32 +208,62 @@ __device__ bool leaf_factor_invert(const double* panel, int kp, double* a, int l
     }
   }
   __syncthreads();
-  // X = U^-1 by columns (one thread each), 8-row panels upward: beyond-panel sums with 8 accumulators, then the
-  // panel's own 8 x 8 back substitution.
+  // X = U^-1 by blocks, on every thread: the eight 8 x 8 diagonal blocks by back substitution (one thread per
+  // column), then neighbouring blocks of s = 8, 16, 32 are joined, X12 = -X11 (U12 X22): T = U12 X22 is written
+  // where X12 goes, then each thread forms its entries of -X11 T in registers before any of them is written back.
+  // (A back substitution per column over the whole block ran its last column's ~1800 dependent FMAs on one thread.)
+  for (int idx = tid; idx < NB * (NB + 1); idx += kThreads) (&X[0][0])[idx] = 0.0;
+  __syncthreads();
   if (tid < NB) {
-    const int c = tid;
-    for (int i0 = (c / P) * P; i0 >= 0; i0 -= P) {
-      double s[P];
+    const int c = tid, p0 = (c / P) * P;
+    double xv[P];
 #pragma unroll
-      for (int ii = 0; ii < P; ++ii) s[ii] = 0.0;
-      for (int q = i0 + P; q <= c; ++q) {
-        const double xq = X[q][c];
+    for (int ii = P - 1; ii >= 0; --ii) {
+      const int r = p0 + ii;
+      double t = 0.0;
 #pragma unroll
-        for (int ii = 0; ii < P; ++ii) s[ii] = fma(U[i0 + ii][q], xq, s[ii]);
-      }
-      double xv[P];
-#pragma unroll
-      for (int ii = P - 1; ii >= 0; --ii) {
-        const int r = i0 + ii;
-        double t = s[ii];
-#pragma unroll
-        for (int jj = ii + 1; jj < P; ++jj) t = fma(U[r][i0 + jj], xv[jj], t);
-        xv[ii] = r > c ? 0.0 : (r == c ? dinv[c] : -dinv[r] * t);
-      }
-#pragma unroll
-      for (int ii = 0; ii < P; ++ii) X[i0 + ii][c] = xv[ii];
+      for (int jj = ii + 1; jj < P; ++jj) t = fma(U[r][p0 + jj], xv[jj], t);
+      xv[ii] = r > c ? 0.0 : (r == c ? dinv[c] : -dinv[r] * t);
     }
-    for (int r = (c / P) * P + P; r < NB; ++r) X[r][c] = 0.0;
+#pragma unroll
+    for (int ii = 0; ii < P; ++ii) X[p0 + ii][c] = xv[ii];
+  }
+  // Each join has NB / 2 rows (pairs x rows of X12): thread (row = tid % 32, group = tid / 32) owns that row's
+  // columns group, group + 4, ..., so one load of the row's entry feeds up to eight independent sums.
+  constexpr int kCols = NB / 2 / 4;  // columns of X12 per thread at the widest join
+  const int jrow = tid % (NB / 2), jgrp = tid / (NB / 2);
+  for (int sz = P; sz < NB; sz *= 2) {
+    const int o = (jrow / sz) * 2 * sz, r = jrow % sz, c0 = o + sz, ncol = sz / 4;
+    __syncthreads();
+    // T = U12 X22 (X22 upper: T(r, c) sums q <= c), written where X12 goes.
+    double acc[kCols];
+#pragma unroll
+    for (int m = 0; m < kCols; ++m) acc[m] = 0.0;
+    for (int q = 0; q < sz; ++q) {
+      const double u = U[o + r][c0 + q];
+#pragma unroll
+      for (int m = 0; m < kCols; ++m) {
+        const int c = jgrp + 4 * m;
+        if (m < ncol && q <= c) acc[m] = fma(u, X[c0 + q][c0 + c], acc[m]);
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < kCols; ++m)
+      if (m < ncol) X[o + r][c0 + jgrp + 4 * m] = acc[m];
+    __syncthreads();
+    // X12 = -X11 T (X11 upper: row r sums q >= r); every entry is formed before any is written back.
+#pragma unroll
+    for (int m = 0; m < kCols; ++m) acc[m] = 0.0;
+    for (int q = r; q < sz; ++q) {
+      const double xr = X[o + r][o + q];
+#pragma unroll
+      for (int m = 0; m < kCols; ++m)
+        if (m < ncol) acc[m] = fma(xr, X[o + q][c0 + jgrp + 4 * m], acc[m]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < kCols; ++m)
+      if (m < ncol) X[o + r][c0 + jgrp + 4 * m] = -acc[m];
   }
   __syncthreads();
   for (int idx = tid; idx < NB * NB; idx += kThreads) {
