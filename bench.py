@@ -69,6 +69,12 @@ def rank_info():
 
 # ------------------------------------------------------------------------------------------------ inputs
 
+def triangle_bytes(n, block=128):
+    """Bytes of one triangle of an n x n FP64 matrix as the library's host-pointer dsygvd moves it: 2D copies of blocks
+    of `block` columns, each with the rows 0 .. (block end - 1) (the diagonal blocks travel whole)."""
+    return 8 * sum(min(n, c0 + block) * (min(n, c0 + block) - c0) for c0 in range(0, n, block))
+
+
 def build_generalized(n, seed):
     """The generalized benchmark pair, built on the host with numpy's default_rng(seed) so that both bench arms (the
     GPU path and the CPU LAPACK chain) solve the same bytes: S = I + G (G_ij = 0.35 exp(-|i-j|/12) u_ij, u ~ U[-1, 1]
@@ -854,7 +860,9 @@ def run_batch_section(args, dev, stream, rank=0, world=1):
         "eigenvalue_error_vs_exact_max": eig_err,
         "mixed": mixed,
         "e2e": {"solves_per_s": round(count / e2e[0], 2), "ms_per_batch": round(e2e[0] * 1e3, 2),
-                "h2d_bytes_per_batch": 2 * elems * 8, "d2h_bytes_per_batch": (2 * elems + sum(sizes)) * 8},
+                "h2d_bytes_per_batch": 2 * sum(triangle_bytes(m) for m in all_sizes[:count]),
+                "d2h_bytes_per_batch": (elems + sum(all_sizes[:count])) * 8
+                + sum(triangle_bytes(m) for m in all_sizes[:count])},
         "l2": "not flushed: the batch's matrices (~%.1f GB) exceed L2" % (4 * elems * 8 / 1e9),
         "input_generation_s": round(gen_s, 1),
         "input_builder": "torch on the device (generator seeded per problem), outside every timed region",
@@ -1080,7 +1088,9 @@ def run_ours(args):
             "stage_share": {k: round(v / total_stage, 3) for k, v in stages},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_ms / world, 4), "unit": "ms",
-                    "h2d_bytes_per_step": 2 * n * n * 8, "d2h_bytes_per_step": (2 * n * n + n) * 8 + 16,
+                    "h2d_bytes_per_step": 2 * triangle_bytes(n),
+                    "d2h_bytes_per_step": (n * n + n) * 8 + triangle_bytes(n) + 16,
+                    "transfers": "H and S up, C (whole), U and w down; H, S and U as their upper triangles",
                     "per_replica_ms": round(e2e_ms, 4)},
             "gpu_launches": int(launches),
             "clocks": clocks,

@@ -62,6 +62,25 @@ def test_sygvd_lower(xe):
     np.testing.assert_allclose(np.tril(l), u_ref.T, atol=1e-12)
 
 
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("n", [90, 300])
+def test_sygvd_host_reads_and_returns_one_triangle(xe, uplo, n):
+    """The host-pointer dsygvd reads only the triangles uplo names and, as LAPACK, leaves B's other triangle as the
+    caller passed it (the transfers move only the referenced triangles): sentinels there change nothing."""
+    h, s, lam = inputs.generalized(n, seed=60 + n)
+    tri = np.triu if uplo == "U" else np.tril
+    other = (lambda x: np.tril(x, -1)) if uplo == "U" else (lambda x: np.triu(x, 1))
+    hs = tri(h) + other(np.full_like(h, 7.5))
+    ss = tri(s) + other(np.full_like(s, -3.25))
+    w, c, f, info = xe.dsygvd(hs, ss, uplo=uplo)
+    assert info == 0
+    np.testing.assert_allclose(w, lam, atol=1e-11)
+    assert metrics.backward_error(h, s, w, c) < 10
+    np.testing.assert_array_equal(other(f), other(ss))
+    u_ref, _ = lapack.potrf_upper(s)
+    np.testing.assert_allclose(tri(f), u_ref if uplo == "U" else u_ref.T, atol=1e-12)
+
+
 def test_config2_generalized_n1204(xe):
     h, s, lam = inputs.generalized(1204, seed=1)
     w_ref, c_ref = lapack.sygvd_chain(h, s)

@@ -957,7 +957,7 @@ using namespace xtbeig;
 
 namespace {
 
-// dsygvd (itype 1, arguments already checked, n > 0) on the calling thread's context: host arrays in, results back.
+// The copy stream and events of host-pointer solves (created on first use).
 bool ensure_copy_stream(Context* c) {
   if (c->copy) return true;
   if (cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) return false;
@@ -966,9 +966,25 @@ bool ensure_copy_stream(Context* c) {
   return true;
 }
 
-// Host-pointer dsygvd.  The transfers overlap the compute on a second stream: B goes first (the Cholesky needs it),
-// A uploads while the Cholesky runs and is symmetrised only when the congruence needs it, and the factor U goes back to
-// the host while the reduction runs.  (With pageable host arrays the driver stages each copy and the overlap is
+// Copies one triangle (with the diagonal) of an n x n column-major matrix, as 2D copies of blocks of 128 columns
+// (upper: rows 0 .. c1-1 of columns c0 .. c1-1; lower: rows c0 .. n-1): about half the bytes of the whole matrix.
+cudaError_t copy_triangle_async(double* dst, int ldd, const double* src, int lds, int n, bool upper, cudaMemcpyKind kind,
+                                cudaStream_t s) {
+  constexpr int kCols = 128;
+  for (int c0 = 0; c0 < n; c0 += kCols) {
+    const int c1 = std::min(n, c0 + kCols);
+    const int r0 = upper ? 0 : c0, r1 = upper ? c1 : n;
+    const cudaError_t err =
+        cudaMemcpy2DAsync(dst + r0 + (size_t)c0 * ldd, sizeof(double) * (size_t)ldd, src + r0 + (size_t)c0 * lds,
+                          sizeof(double) * (size_t)lds, sizeof(double) * (size_t)(r1 - r0), (size_t)(c1 - c0), kind, s);
+    if (err != cudaSuccess) return err;
+  }
+  return cudaSuccess;
+}
+
+// Host-pointer dsygvd (itype 1, arguments already checked, n > 0) on the calling thread's context.  The transfers
+// overlap the compute on a second stream: B goes first (the Cholesky needs it), A uploads while the Cholesky runs and
+// is symmetrised only when the congruence needs it, and the factor U goes back to the host while the reduction runs.  Only the triangles named by uplo travel in either direction.  (With pageable host arrays the driver stages each copy and the overlap is
 // smaller; pinned arrays overlap fully.)
 int sygvd_host(char jz, char ul, int n, double* a, int lda, double* b, int ldb, double* w) {
   Context* c = context();
@@ -986,23 +1002,27 @@ int sygvd_host(char jz, char ul, int n, double* a, int lda, double* b, int ldb, 
     // The copy stream starts after everything queued on the compute stream so far (buffer reuse across calls).
     k.check(cudaEventRecord(c->ev_out, k.s), "event");
     if (k.ok()) k.check(cudaStreamWaitEvent(cs, c->ev_out, 0), "wait");
-    if (k.ok()) k.check(cudaMemcpyAsync(db, b, sizeof(double) * (size_t)ldb * n, cudaMemcpyHostToDevice, cs), "H2D B");
+    // Only the referenced triangles of B and A travel (the solve reads nothing else).
+    if (k.ok()) k.check(copy_triangle_async(db, ldb, b, ldb, n, ul == 'U', cudaMemcpyHostToDevice, cs), "H2D B");
     if (k.ok()) k.check(cudaEventRecord(c->ev_in_b, cs), "event");
-    if (k.ok()) k.check(cudaMemcpyAsync(da, a, sizeof(double) * (size_t)lda * n, cudaMemcpyHostToDevice, cs), "H2D A");
+    if (k.ok()) k.check(copy_triangle_async(da, lda, a, lda, n, ul == 'U', cudaMemcpyHostToDevice, cs), "H2D A");
     if (k.ok()) k.check(cudaEventRecord(c->ev_in_a, cs), "event");
     if (k.ok()) k.check(cudaStreamWaitEvent(k.s, c->ev_in_b, 0), "wait B");
   }
   if (k.ok()) {
-    if (ul == 'U') copy_matrix<double>(n, n, db, ldb, du, n, k.s);
+    // Only B's triangle is on the device: the factor's work copy is the symmetric matrix it defines.
+    if (ul == 'U') symmetrize_upper<double>(n, db, ldb, du, n, k.s);
     else symmetrize_lower<double>(n, db, ldb, du, n, k.s);
   }
   k.after_factor = [&](Call& kk) {
-    // U is final: put it into the caller's triangle of B and send it back on the copy stream.
-    if (ul == 'U') copy_matrix<double>(n, n, du, n, db, ldb, kk.s);
+    // U is final: put it into the caller's triangle of B (the other triangle's uploaded entries stay, so the copy
+    // back returns them unchanged) and send it back on the copy stream.
+    if (ul == 'U') copy_upper<double>(n, du, n, db, ldb, kk.s);
     else upper_transpose_to_lower<double>(n, du, n, db, ldb, kk.s);
     kk.check(cudaEventRecord(c->ev_factor, kk.s), "event");
     if (kk.ok()) kk.check(cudaStreamWaitEvent(cs, c->ev_factor, 0), "wait U");
-    if (kk.ok()) kk.check(cudaMemcpyAsync(b, db, sizeof(double) * (size_t)ldb * n, cudaMemcpyDeviceToHost, cs), "D2H B");
+    // The factor's triangle only: LAPACK leaves the other triangle of B as the caller passed it.
+    if (kk.ok()) kk.check(copy_triangle_async(b, ldb, db, ldb, n, ul == 'U', cudaMemcpyDeviceToHost, cs), "D2H B");
     // H for the congruence.
     if (kk.ok()) kk.check(cudaStreamWaitEvent(kk.s, c->ev_in_a, 0), "wait A");
     if (kk.ok()) {

@@ -80,6 +80,9 @@ void mirror_upper_inplace(int n, T* a, int lda, cudaStream_t s);
 // B = A (m x n), column-major with leading dimensions.
 template <typename T>
 void copy_matrix(int m, int n, const T* a, int lda, T* b, int ldb, cudaStream_t s);
+// b's upper triangle (with the diagonal) <- a's; b's strict lower triangle is not touched.
+template <typename T>
+void copy_upper(int n, const T* a, int lda, T* b, int ldb, cudaStream_t s);
 template <typename T>
 void set_identity(int n, T* a, int lda, cudaStream_t s);
 template <typename T>

@@ -85,6 +85,16 @@ __global__ void copy_kernel(int m, int n, const T* __restrict__ a, int lda, T* _
   }
 }
 
+// The upper triangle (with the diagonal) of an n x n matrix; b's strict lower triangle is left as it is.
+template <typename T>
+__global__ void copy_upper_kernel(int n, const T* __restrict__ a, int lda, T* __restrict__ b, int ldb) {
+  const size_t total = (size_t)n * n;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % n), j = (int)(idx / n);
+    if (i <= j) b[i + (size_t)j * ldb] = a[i + (size_t)j * lda];
+  }
+}
+
 template <typename T>
 __global__ void identity_kernel(int n, T* a, int lda) {
   const size_t total = (size_t)n * n;
@@ -156,6 +166,12 @@ void mirror_upper_inplace(int n, T* a, int lda, cudaStream_t s) {
 }
 
 template <typename T>
+void copy_upper(int n, const T* a, int lda, T* b, int ldb, cudaStream_t s) {
+  if (n <= 0) return;
+  copy_upper_kernel<T><<<grid_for((size_t)n * n), 256, 0, s>>>(n, a, lda, b, ldb); note_launches();
+}
+
+template <typename T>
 void copy_matrix(int m, int n, const T* a, int lda, T* b, int ldb, cudaStream_t s) {
   if (m <= 0 || n <= 0) return;
   copy_kernel<T><<<grid_for((size_t)m * n), 256, 0, s>>>(m, n, a, lda, b, ldb); note_launches();
@@ -203,6 +219,7 @@ template void symmetrize_upper<float>(int, const float*, int, float*, int, cudaS
 template void symmetrize_lower<double>(int, const double*, int, double*, int, cudaStream_t);
 template void symmetrize_lower<float>(int, const float*, int, float*, int, cudaStream_t);
 template void upper_transpose_to_lower<double>(int, const double*, int, double*, int, cudaStream_t);
+template void copy_upper<double>(int, const double*, int, double*, int, cudaStream_t);
 template void mirror_upper_inplace<double>(int, double*, int, cudaStream_t);
 template void mirror_upper_inplace<float>(int, float*, int, cudaStream_t);
 template void copy_matrix<double>(int, int, const double*, int, double*, int, cudaStream_t);
