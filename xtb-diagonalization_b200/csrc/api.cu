@@ -620,8 +620,16 @@ void stage_factor(Call& k, int n, double* u, int ldu, double* x, int ldx) {
   if (!k.ok() || n <= 0) return;
   double* t = k.template dev<double>("gv.T", (size_t)n * n);
   unsigned* pctr = k.template dev<unsigned>("potrf.ctr", 64);
+  // Inside a batch the Cholesky of one problem would take every SM while its one-CTA diagonal leaf sets the pace: it
+  // takes enough CTAs for its first trailing update to keep up with the leaf (about six 64 x 64 tiles per CTA per
+  // step) and leaves the other SMs to the problems beside it.  U and X do not depend on the grid.
+  int grid = k.c->num_sms;
+  if (t_plan.batch_grid == 1) {
+    const int nt = (n + 63) / 64;
+    grid = std::min(grid, std::max(4, (nt * (nt - 1) / 2 + 5) / 6));
+  }
   if (k.ok())
-    k.check(potrf_inverse_upper(n, u, ldu, x, ldx, t, pctr, k.c->num_sms, k.c->d_status, wait_limit_ns(), k.s),
+    k.check(potrf_inverse_upper(n, u, ldu, x, ldx, t, pctr, grid, k.c->d_status, wait_limit_ns(), k.s),
             "potrf+inverse");
   k.mark("potrf_inverse");
   if (k.after_factor && k.ok()) k.after_factor(k);
