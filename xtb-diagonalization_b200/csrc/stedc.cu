@@ -80,6 +80,8 @@ struct DcBufs {
 };
 
 constexpr double kEps = 1.1102230246251565e-16;
+constexpr int kSecularWarps = 4;       // warps per secular root at levels with merges of at least kSecularGroupMin
+constexpr int kSecularGroupMin = 512;
 
 // Ordering key: NaN sorts as +inf, so every ranking below is a bijection even on non-finite input (a failed earlier
 // stage must never turn into an out-of-range index).
@@ -535,30 +537,54 @@ struct SecSums {
   double psi, dpsi, phi, dphi, asum;
 };
 
-__device__ __forceinline__ SecSums sec_eval(const double* dl, const double* z, int K, int o, int a, double tau) {
-  const int lane = threadIdx.x & 31;
+// A root is solved by WPR warps together (one CTA of 32 WPR threads when WPR > 1): every sum runs over the poles
+// strided by the group's threads, then across its warps in warp order through shared memory (sh: 2 x 5 x WPR doubles,
+// alternating by `tog`, so one __syncthreads per sum; every thread receives the same value).
+template <int WPR>
+__device__ __forceinline__ void group_sums(double* v, int cnt, double* sh, int& tog) {
+#pragma unroll 5
+  for (int j = 0; j < cnt; ++j) v[j] = warp_sum(v[j]);
+  if constexpr (WPR > 1) {
+    double* buf = sh + tog * 5 * WPR;
+    tog ^= 1;
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+      for (int j = 0; j < cnt; ++j) buf[j * WPR + w] = v[j];
+    __syncthreads();
+    for (int j = 0; j < cnt; ++j) {
+      double r = 0.0;
+#pragma unroll
+      for (int q = 0; q < WPR; ++q) r += buf[j * WPR + q];
+      v[j] = r;
+    }
+  }
+}
+
+template <int WPR>
+__device__ __forceinline__ SecSums sec_eval(const double* dl, const double* z, int K, int o, int a, double tau,
+                                            double* sh, int& tog) {
+  const int lane = threadIdx.x & (32 * WPR - 1);
   SecSums r{0, 0, 0, 0, 0};
   const double dlo = dl[o];
-  for (int i = lane; i < K; i += 32) {
+  for (int i = lane; i < K; i += 32 * WPR) {
     const double del = (dl[i] - dlo) - tau;
     const double inv = 1.0 / del;
     const double t = z[i] * z[i] * inv;
     if (i <= a) { r.psi += t; r.dpsi += t * inv; } else { r.phi += t; r.dphi += t * inv; }
     r.asum += fabs(t);
   }
-  r.psi = warp_sum(r.psi);
-  r.dpsi = warp_sum(r.dpsi);
-  r.phi = warp_sum(r.phi);
-  r.dphi = warp_sum(r.dphi);
-  r.asum = warp_sum(r.asum);
-  return r;
+  double v[5] = {r.psi, r.dpsi, r.phi, r.dphi, r.asum};
+  group_sums<WPR>(v, 5, sh, tog);
+  return SecSums{v[0], v[1], v[2], v[3], v[4]};
 }
 
 // Root j of 1/rho + sum_i z_i^2 / (dl_i - lambda) = 0 (rho > 0, dl ascending): lambda = dl[o] + tau.
 // Returns false if it did not converge within the iteration limit (the best iterate is still returned).
+template <int WPR>
 __device__ bool secular_root(const double* dl, const double* z, int K, double rho, int j, int* o_out,
-                             double* tau_out) {
-  const int lane = threadIdx.x & 31;
+                             double* tau_out, double* sh) {
+  const int lane = threadIdx.x & (32 * WPR - 1);
+  int tog = 0;
   const double rinv = 1.0 / rho;
   if (K == 1) {
     *o_out = 0;
@@ -570,15 +596,16 @@ __device__ bool secular_root(const double* dl, const double* z, int K, double rh
   if (j < K - 1) {
     const double dj = dl[j], gap = dl[j + 1] - dj;
     double fm = 0.0;
-    for (int i = lane; i < K; i += 32) fm += z[i] * z[i] / ((dl[i] - dj) - 0.5 * gap);
-    fm = rinv + warp_sum(fm);
+    for (int i = lane; i < K; i += 32 * WPR) fm += z[i] * z[i] / ((dl[i] - dj) - 0.5 * gap);
+    group_sums<WPR>(&fm, 1, sh, tog);
+    fm = rinv + fm;
     if (fm >= 0.0) { o = j; lo = 0.0; hi = 0.5 * gap; }
     else { o = j + 1; lo = -0.5 * gap; hi = 0.0; }
     a = j;
   } else {
     double zz = 0.0;
-    for (int i = lane; i < K; i += 32) zz += z[i] * z[i];
-    zz = warp_sum(zz);
+    for (int i = lane; i < K; i += 32 * WPR) zz += z[i] * z[i];
+    group_sums<WPR>(&zz, 1, sh, tog);
     o = K - 1;
     lo = 0.0;
     hi = rho * zz;
@@ -590,7 +617,7 @@ __device__ bool secular_root(const double* dl, const double* z, int K, double rh
   double tau = 0.5 * (lo + hi);
   bool conv = false;
   for (int it = 0; it < 120; ++it) {
-    const SecSums S = sec_eval(dl, z, K, o, a, tau);
+    const SecSums S = sec_eval<WPR>(dl, z, K, o, a, tau, sh, tog);
     const double f = rinv + S.psi + S.phi;
     const double errb = 8.0 * kEps * (rinv + S.asum) + kEps * fabs(tau) * (S.dpsi + S.dphi);
     if (fabs(f) <= errb) { conv = true; break; }
@@ -645,9 +672,40 @@ __global__ void dc_secular_kernel(DcBufs B) {
   const double* z = B.zk + s;
   int o;
   double tau;
-  const bool ok = secular_root(dl, z, K, inf.rho, j, &o, &tau);
+  const bool ok = secular_root<1>(dl, z, K, inf.rho, j, &o, &tau, nullptr);
   if (!ok && lane == 0) set_status(B.st, kStatusSecularNoConv, s + j + 1, s);
   if (lane == 0) {
+    B.rorg[s + j] = o;
+    B.rtau[s + j] = tau;
+    B.lam[s + j] = dl[o] + tau;
+  }
+}
+
+// The same with WPR warps per root (one CTA per global position), for levels whose merges are large: each evaluation
+// of the secular function then loops over K / (32 WPR) poles per thread instead of K / 32.  The early exits depend
+// only on the CTA's position (the status word is read once and shared), so all its threads meet every __syncthreads.
+template <int WPR>
+__global__ void __launch_bounds__(32 * WPR) dc_secular_group_kernel(DcBufs B) {
+  __shared__ double sh[2 * 5 * WPR];
+  __shared__ int s_failed;
+  const int gw = blockIdx.x;
+  if (gw >= B.n) return;
+  if (threadIdx.x == 0) s_failed = ld_volatile_i32(&B.st->code);
+  __syncthreads();
+  if (s_failed != 0) return;
+  const int mi = B.posMerge[gw];
+  if (mi < 0) return;
+  const MergeDesc md = B.merges[mi];
+  const MergeInfo inf = B.info[mi];
+  const int s = md.s, j = gw - s, K = inf.K;
+  if (j >= K) return;
+  const double* dl = B.dlam + s;
+  const double* z = B.zk + s;
+  int o;
+  double tau;
+  const bool ok = secular_root<WPR>(dl, z, K, inf.rho, j, &o, &tau, sh);
+  if (threadIdx.x == 0) {
+    if (!ok) set_status(B.st, kStatusSecularNoConv, s + j + 1, s);
     B.rorg[s + j] = o;
     B.rtau[s + j] = tau;
     B.lam[s + j] = dl[o] + tau;
@@ -995,7 +1053,11 @@ cudaError_t stedc_device(int n, double* d, double* e, double* z, int ldz, void* 
     dc_gather_kernel<<<dim3(nm, (maxn + 127) / 128, (maxn + 31) / 32), 128, 0, s>>>(B); note_launches();
     const int warps_per_block = 8;
     const int nblk = (n + warps_per_block - 1) / warps_per_block;
-    dc_secular_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();
+    if (maxn >= kSecularGroupMin) {
+      dc_secular_group_kernel<kSecularWarps><<<n, 32 * kSecularWarps, 0, s>>>(B); note_launches();
+    } else {
+      dc_secular_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();
+    }
     dc_zhat_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();
     dc_vectors_kernel<<<nblk, 32 * warps_per_block, 0, s>>>(B); note_launches();
     const bool partial = l == L - 1 && m_cols < n;  // the top merge forms only the wanted columns
