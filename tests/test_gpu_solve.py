@@ -81,6 +81,26 @@ def test_sygvd_host_reads_and_returns_one_triangle(xe, uplo, n):
     np.testing.assert_allclose(tri(f), u_ref if uplo == "U" else u_ref.T, atol=1e-12)
 
 
+@pytest.mark.parametrize("n", [1100, 1600])
+def test_host_solve_matches_device_solve(xe, n):
+    """From n = 1024 the host-pointer dsygvd computes C = (X Q) Z in column blocks and copies each to the host while
+    the next is formed; the eigenvectors and eigenvalues are bit for bit those of the device-pointer solve."""
+    import torch
+
+    h, s, lam = inputs.generalized(n, seed=80 + n)
+    w, c, u, info = xe.dsygvd(h, s)
+    assert info == 0
+    dev = torch.device("cuda", 0)
+    xe.set_device(0)
+    H = torch.from_numpy(np.asfortranarray(h).T.copy()).to(dev)  # row-major storage of H^T = H: column-major H
+    S = torch.from_numpy(np.asfortranarray(s).T.copy()).to(dev)
+    W = torch.empty(n, dtype=torch.float64, device=dev)
+    assert xe.dsygvd_device(n, H.data_ptr(), n, S.data_ptr(), n, W.data_ptr()) == 0
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(W.cpu().numpy(), w)
+    np.testing.assert_array_equal(H.cpu().numpy().T, c)
+
+
 def test_config2_generalized_n1204(xe):
     h, s, lam = inputs.generalized(1204, seed=1)
     w_ref, c_ref = lapack.sygvd_chain(h, s)

@@ -226,6 +226,11 @@ struct Call {
   bool timing = false;
   // Called by the generalized pipelines right after the Cholesky factor U is final and before the first read of H.
   std::function<void(Call&)> after_factor;
+  // Set by host-pointer solves: called after each column block [c0, c1) of the final FP64 eigenvectors is written (the
+  // back-transformation then runs in column blocks, so that their copies to the host overlap the rest); the stage
+  // sets columns_sent when it did so.
+  std::function<void(Call&, int, int)> on_columns;
+  bool columns_sent = false;
 
   // Host-pointer calls run on the context's own stream; device-pointer calls on the caller's stream, where NULL is the
   // CUDA legacy default stream (ordered with the caller's other work on blocking streams).
@@ -557,12 +562,20 @@ bool use_xq(Call& k, int n) {
 
 // The C = (X Q) Z step after the tridiagonal eigensolve: waits for the aux stream's X Q, then one GEMM.
 template <typename T>
-void stage_xq_backtransform(Call& k, int n, int cols, const T* m, const T* z, T* c, const TcGemm& tc) {
+void stage_xq_backtransform(Call& k, int n, int cols, const T* m, const T* z, T* c, const TcGemm& tc,
+                            bool final_c = false) {
   if (!k.ok()) return;
   k.check(cudaStreamWaitEvent(k.s, k.c->ev_join, 0), "join");
   k.mark("xq_join");
-  GemmDesc<T> p = gemm_problem<T>(n, cols, n, T(1), m, n, 0, z, n, 0, T(0), c, n);
-  if (k.ok()) k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "C = (X Q) Z");
+  // Column blocks of at least 512 (the width the Ozaki engine takes), at most 3, when a caller copies C out as it goes.
+  const int nblk = (final_c && k.on_columns) ? std::max(1, std::min(3, cols / 512)) : 1;
+  for (int b = 0; b < nblk && k.ok(); ++b) {
+    const int c0 = (int)((long long)cols * b / nblk), c1 = (int)((long long)cols * (b + 1) / nblk);
+    GemmDesc<T> p = gemm_problem<T>(n, c1 - c0, n, T(1), m, n, 0, z + (size_t)c0 * n, n, 0, T(0), c + (size_t)c0 * n, n);
+    k.check(gemm_run(k.c->arena, tc, &p, 1, k.s), "C = (X Q) Z");
+    if (nblk > 1 && k.ok()) k.on_columns(k, c0, c1);
+  }
+  if (nblk > 1 && k.ok()) k.columns_sent = true;
   k.mark("backtransform");
 }
 
@@ -662,7 +675,7 @@ void solve_factored_fp64(Call& k, int n, double* h, const double* x, int ldx, do
   stage_stedc(k, n, w, e, z, n, mv);
   k.mark("stedc");
   if (red.xq) {
-    stage_xq_backtransform<double>(k, n, mv, mx, z, c, tc);
+    stage_xq_backtransform<double>(k, n, mv, mx, z, c, tc, true);
     return;
   }
   stage_backtransform<double>(k, "gv.", n, mv, red, z, n, tc);
@@ -1038,10 +1051,22 @@ int sygvd_host(char jz, char ul, int n, double* a, int lda, double* b, int ldb, 
       else symmetrize_lower<double>(n, da, lda, dh, n, kk.s);
     }
   };
+  if (jz == 'V') {
+    // C's column blocks go to the host on the copy stream as the back-transformation writes them.
+    k.on_columns = [&](Call& kk, int c0, int c1) {
+      kk.check(cudaEventRecord(c->ev_factor, kk.s), "event");
+      if (kk.ok()) kk.check(cudaStreamWaitEvent(cs, c->ev_factor, 0), "wait C");
+      if (kk.ok())
+        kk.check(cudaMemcpy2DAsync(a + (size_t)c0 * lda, sizeof(double) * lda, dc + (size_t)c0 * n,
+                                   sizeof(double) * n, sizeof(double) * n, c1 - c0, cudaMemcpyDeviceToHost, cs),
+                 "D2H C block");
+    };
+  }
   core_sygvd(k, n, dh, du, dc, dw);
   k.after_factor = nullptr;
+  k.on_columns = nullptr;
   k.d2h(w, dw, sizeof(double) * n, "D2H w");
-  if (jz == 'V' && k.ok())
+  if (jz == 'V' && k.ok() && !k.columns_sent)
     k.check(cudaMemcpy2DAsync(a, sizeof(double) * lda, dc, sizeof(double) * n, sizeof(double) * n, n,
                               cudaMemcpyDeviceToHost, k.s), "D2H C");
   // The compute stream's completion covers the copy stream's work; after a failure, no copy may still be reading or
